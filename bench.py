@@ -1,0 +1,280 @@
+"""RK4 steps/s of the HF-GKBA G1-G2 propagation at Ns=16, Nb=2 (n=32) on B200.
+
+Workload (the configuration the headline metric is quoted on): Hubbard chain
+Ns=16, Nb=2, t1=1, t2=0.3, U=1.5, EHM with w(r)=U/(1+r), full quench 1.5 on
+Nq=4 sites, dt=0.01.  Initial state: make_G0, then the adiabatic switching
+phase (untimed); a "step" is one RK4 step (4 stages) of the propagation.
+
+Arms:
+  default            the library (C ABI via ctypes) on cuda:LOCAL_RANK; one
+                     independent replica per rank ("replicas only": a single
+                     system does not shard), value = all ranks' steps / max time.
+  --impl reference   the reference's own OpenMP CPU build (oracle/_ref/g12_ref,
+                     compiled from the reference headers) on the host cores,
+                     RK4 steps of the same workload; rank 0 only.
+
+Timing: device time of the K timed steps from CUDA events on the library's
+stream (synchronised on both sides), max over ranks; the working set (2 x 5
+tensors of 16 MB) exceeds the 126 MB L2.  e2e: the same K steps through the
+C ABI from host buffers (state upload, per-step G1 snapshots copied back,
+state download), wall clock.
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = dict(Ns=16, Nb=2, Nq=4, time_steps=10000, U=1.5, t1=1.0, t2=0.3, dt=0.01, EHM=True,
+                v_law="inv", q_type="full", quench_strength=1.5)
+METRIC = "RK4 steps/s at Ns=16,Nb=2: mixed/learned vs plain FP64 on B200, G1 err<=1e-6"
+CONFIG = {"workload": "HF-GKBA GW, Hubbard chain Ns=16 Nb=2 (n=32), EHM w(r)=U/(1+r), U=1.5, t2=0.3, "
+                      "full quench 1.5 on Nq=4, dt=0.01",
+          "n": 32, "g2_entries_per_tensor": 32 ** 4, "l2_policy": "working set 160 MB > 126 MB L2"}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi") is None:
+            return self
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits", "-lms", "100"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def allmax(pg, v):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reference_cpu(steps, warmup, max_seconds=None):
+    """Times the compiled reference (OpenMP, all host cores) on RK4 steps of the
+    workload.  Returns (steps/s, cores, sample description, per-step seconds)."""
+    from oracle import REF_EXE, Config
+    cores = os.cpu_count() or 1
+    cfg = Config(Ns=16, Nb=2, Nq=4, time_steps=10000, U=1.5, t1=1.0, t2=0.3, dt=0.01, EHM=True, vlaw="inv",
+                 q_type="full", quench_strength=1.5)
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    if not os.path.exists(REF_EXE):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "input"), "w") as f:
+            f.write(cfg.input_text())
+        if max_seconds is not None:
+            # size the sample: one step first, then as many as fit
+            r = subprocess.run([REF_EXE, "--vlaw", "inv", "--time-rk", "0", "1"], cwd=d, env=env,
+                               capture_output=True, text=True, check=True)
+            one = json.loads(r.stdout.strip().splitlines()[-1])["seconds"]
+            steps = int(max(2, min(steps, max_seconds / max(one, 1e-3))))
+            warmup = 0
+        r = subprocess.run([REF_EXE, "--vlaw", "inv", "--time-rk", str(warmup), str(steps)], cwd=d, env=env,
+                           capture_output=True, text=True, check=True)
+    js = json.loads(r.stdout.strip().splitlines()[-1])
+    sps = js["rk_iterations"] / js["seconds"]
+    sample = (f"{js['rk_iterations']} RK4 steps of the n=32 workload after {warmup} warm-up steps, "
+              f"reference OpenMP build (oracle/_ref/g12_ref), OMP_NUM_THREADS={cores}")
+    return sps, cores, sample, js["seconds"] / js["rk_iterations"]
+
+
+def run_reference_arm(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    res = reference_cpu(args.steps, args.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "compiled reference oracle/_ref/g12_ref not built"}))
+        return
+    sps, cores, sample, _ = res
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": sps, "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / sps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (physics-defined input)",
+        "config": dict(CONFIG, parallelism="OpenMP CPU, rank 0"),
+        "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "bf16x3"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    world, rank, local, pg = dist_setup(args.gpus)
+    import g12kba_b200 as g12
+    p = g12.make_params(**WORKLOAD)
+    n = p.n
+    G0 = g12.make_G0(p)
+
+    # prepared state: adiabatic switching (untimed), then the timed RK4 steps
+    def prepared(prec):
+        ctx = g12.Context(p, prec, local)
+        ctx.set_state(G0)
+        ctx.adiabatic_switch()
+        return ctx
+
+    ctx = prepared(args.precision)
+    state = ctx.get_state()
+    ctx.propagate_dipole(args.warmup)
+    barrier(pg)
+    with Clocks(local) as clk:
+        _, rc = ctx.propagate_dipole(args.steps)
+        dev_ms = ctx.last_device_ms
+    barrier(pg)
+    ms = allmax(pg, dev_ms)
+    value = world * args.steps / (ms / 1e3)
+    launches = ctx.launches_per_step * args.steps
+
+    # e2e through the C ABI with host buffers
+    traj_host = np.zeros((args.steps, n, n), np.complex128)
+    barrier(pg)
+    t0 = time.perf_counter()
+    ctx.set_state(*state)
+    t_mid = time.perf_counter()
+    import ctypes
+    done = ctypes.c_int64()
+    g12.lib().g12_propagate(ctx.h, args.steps, traj_host.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                            ctypes.byref(done))
+    out = ctx.get_state()
+    t1 = time.perf_counter()
+    e2e_s = allmax(pg, t1 - t0)
+    state_bytes = (n * n + 2 * n ** 4) * 16
+    e2e = {"value": world * args.steps / e2e_s, "unit": "steps/s",
+           "h2d_bytes_per_step": state_bytes / args.steps,
+           "d2h_bytes_per_step": n * n * 16 + state_bytes / args.steps,
+           "note": "set_state + propagate(K, per-step G1 snapshots to host) + get_state, wall clock"}
+
+    # per-kernel device times (CUDA events on the library stream), roofline of the top kernel
+    kt = ctx.kernel_times(2)
+    ctx.close()
+    tot = sum(a * c for a, c in kt.values())
+    top = max(kt, key=lambda k: kt[k][0] * kt[k][1])
+    top_ms = kt[top][0]
+    fp64_peak = g12.fp64_peak_tflops(local)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+    # one k_apply launch: both tensors, one stage, two of the four mode products:
+    # 2 * 2 * n^5 complex MACs * 8 flops; algorithmic bytes: half of the stage's
+    # 5 state passes over 2 tensors (640 n^4 B per step / 8 apply launches)
+    flops = 32.0 * n ** 5
+    bytes_alg = 80.0 * n ** 4
+    roofline = {"bound": "fp64", "kernel": top, "achieved": flops / (top_ms * 1e-3) / 1e12,
+                "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": flops / (top_ms * 1e-3) / 1e12 / fp64_peak, "traffic": None,
+                "peak_source": "measured FP64 FMA probe (g12_fp64_peak_tflops) on this GPU",
+                "hbm_achieved_gbs": bytes_alg / (top_ms * 1e-3) / 1e9, "hbm_peak_gbs": peaks.get("hbm_gbs"),
+                "hbm_frac": bytes_alg / (top_ms * 1e-3) / 1e9 / peaks.get("hbm_gbs", 6650.0)}
+    kernels = {k: {"ms_per_launch": a, "launches_per_step": c, "share": a * c / tot} for k, (a, c) in kt.items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = reference_cpu(8, 0, max_seconds=20.0)
+        if res is not None:
+            sps, cores, sample, _ = res
+            cpu = {"value": sps, "unit": "steps/s", "cores": cores, "kind": "reference", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else args.precision,
+            "data": "synthetic (physics-defined input: make_G0 + adiabatic switching)",
+            "config": dict(CONFIG, precision=args.precision, parallelism=f"replicas x{world}"),
+            "status": rc, "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "kernels": kernels,
+            "cpu_baseline": cpu, "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

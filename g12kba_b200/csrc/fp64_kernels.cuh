@@ -1,0 +1,545 @@
+// FP64 device kernels of one RK4 stage of the HF-GKBA G1-G2 equations
+// (reference: G12KBA-GW/src/headers/{HF,commutators,psi,pi,collision_integral,
+// G1_G2_t_step,RK_solver,AS}.h).
+//
+// Device layout (per system, n = Ns*Nb, orbital mu = site + band*Ns):
+//   G1-like arrays: n x n row-major, element [mu][nu] at nu + n*mu.
+//   G2 tensors:     x = nu1 + n*nu2 + n^2*mu1 + n^3*mu2 for G2[mu1 mu2; nu1 nu2]
+//                   (the reference's IDX_8D with sites and bands regrouped into
+//                   orbitals; identical to it for Nb = 1).  Tensor 0 is G2xxxx,
+//                   tensor 1 is G2xyxy, stored back to back.
+//   D[t][a][b][r] = G2_t[a, r; b, r]   (n^3, the particle-2 diagonal)
+//   Q[t][a][b][r]                        (n^3, Pi factor, see k_prep)
+//   Rt[a][b][s]                          (n^2*Ns, Psi factor, see k_prep)
+//
+// Factorisation used here (derived from the reference loops, not copied):
+//   Pi(psi.h/pi.h notation) = G1[mu2][nu2] * (Q[mu1][nu1][mu2] - Q[mu1][nu1][nu2])
+//   Q_t[a][b][(s,r)] = -i*U*(S[a][b][s] - D_t'[a][b][(s,r)]) - i*Vp[a][b][s]
+//       S[s] = sum_r (Dxx + Dxy)[(s,r)],  Vp[s] = sum_m V_m (S[s+m] + S[s-m]),
+//       t' = xx for Pi_xx (pi.h called with G2xy, G2xx) and xy for Pi_xy.
+//   collision_int I[mu][nu] = Q_xx[mu][nu][mu].
+//   Psi_xy = g11 g22 (W(i,j) - W(k,l)) + i g22 (Rt[mu1][nu1][j] - Rt[mu1][nu1][l])
+//                                      + i g11 (Rt[mu2][nu2][i] - Rt[mu2][nu2][k])
+//       W(s,s') = U [s=s'] + V_|s-s'|,  Rt[a][b][s] = U R[s] + sum_m V_m (R[s+m] + R[s-m]),
+//       R[a][b][s] = sum_r G1[a][(s,r)] G1[(s,r)][b].
+//   Psi_xx = Psi_xy - U g11 g22 ([mu1=mu2] - [nu1=nu2])
+//            - i U g22 (G1[mu1][mu2]G1[mu2][nu1] - G1[mu1][nu2]G1[nu2][nu1])
+//            - i U g11 (G1[mu2][mu1]G1[mu1][nu2] - G1[mu2][nu1]G1[nu1][nu2]).
+//   Two-body commutator C = H2 M - M H2 with M = G2 as an n^2 x n^2 matrix and
+//   H2 = h (x) 1 + 1 (x) h: k_apply<false> (rows: particle indices mu1, mu2) and
+//   k_apply<true> (columns nu1, nu2); each is Y = L X + X R on a batch of n x n
+//   matrices X, with (L, R) = (h, h^T) or (h^T, h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace g12 {
+
+constexpr int kMaxN = 64;
+
+struct Dev {
+    int Ns, Nb, n, nv, gate, debug;
+    long long n2, n3, n4;
+    double t1, t2;
+    double law[kMaxN];  // V_m = U_eff * law[m-1], m = 1..nv
+    double2 *Y1, *G1t0, *G1t1, *RK1, *h, *Ix, *comm_dbg, *K1_dbg;
+    double2 *Y2, *RK2, *TMP0, *TMP1, *TAB, *D, *Q, *Rt;
+    double2 *traj;
+    double *dip;
+    long long traj_cap;
+    const StepP *sched;
+    long long *counter, *limit;
+    int *status, *active;
+    StepP *cur;
+};
+
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 c_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 c_conj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 c_i(double2 a) { return make_double2(-a.y, a.x); }    // i*a
+__device__ __forceinline__ double2 c_mi(double2 a) { return make_double2(a.y, -a.x); }   // -i*a
+__device__ __forceinline__ double2 c_mac(double2 acc, double2 a, double2 b)
+{
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+    return acc;
+}
+
+__device__ __forceinline__ const double2 *g1_stage(const Dev &d, int k) { return (k & 1) ? d.G1t1 : d.G1t0; }
+__device__ __forceinline__ double2 *g1_next(const Dev &d, int k) { return (k & 1) ? d.G1t0 : d.G1t1; }
+// stage k reads Y (k = 0) or TMP[(k+1)&1]; stage k < 3 writes TMP[k&1]
+__device__ __forceinline__ const double2 *g2_stage(const Dev &d, int k)
+{
+    return k == 0 ? d.Y2 : (((k + 1) & 1) ? d.TMP1 : d.TMP0);
+}
+__device__ __forceinline__ double2 *g2_next(const Dev &d, int k) { return (k & 1) ? d.TMP1 : d.TMP0; }
+
+// ---------------------------------------------------------------------------
+// Step head (RK_solver.h:98-110): copy this step's scalars, record the
+// snapshot and dipole, apply the site-0 density guard, stage-0 G1 input.
+__global__ void k_step_begin(Dev d)
+{
+    __shared__ long long s_step;
+    __shared__ int s_act, s_rec;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        long long s = *d.counter;
+        int act = (*d.status == 0) && (s < *d.limit);
+        int rec = 0;
+        if (act) {
+            *d.cur = d.sched[s];
+            rec = d.sched[s].record;
+        }
+        s_step = s;
+        s_act = act;
+        s_rec = rec;
+    }
+    __syncthreads();
+    if (!s_act) {
+        if (tid == 0) *d.active = 0;
+        return;
+    }
+    const int n = d.n;
+    const long long s = s_step;
+    double2 *tr = d.traj + (s % d.traj_cap) * d.n2;
+    for (int x = tid; x < n * n; x += blockDim.x) {
+        double2 v = d.Y1[x];
+        d.G1t0[x] = v;
+        if (s_rec) tr[x] = v;
+    }
+    if (s_rec && tid < 32) {
+        // dipole.h:25-32, warp-shuffle reduction over the mirrored diagonal
+        const double sq = double(n);
+        double acc = 0.0;
+        for (int i = tid; i < n / 2; i += 32)
+            acc += 2 * (sq / 2 - i - .5) * (d.Y1[i * (n + 1)].y - d.Y1[n * n - i * (n + 1) - 1].y) / sq;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (tid == 0) d.dip[s % d.traj_cap] = acc;
+    }
+    if (tid == 0) {
+        int act = 1;
+        if (s_rec) {
+            double nd = 2 * d.Y1[0].y;
+            if (fabs(nd) > 3 || isnan(nd)) {
+                *d.status = int(s + 1);
+                act = 0;
+            }
+        }
+        *d.active = act;
+        *d.counter = s + 1;
+    }
+}
+
+// HF.h:57-104, entry by entry.
+__device__ double2 h_entry(const Dev &d, const double2 *G, int mu, int nu, const StageP &st)
+{
+    const int Ns = d.Ns, n = d.n;
+    const int i = mu % Ns, a = mu / Ns, j = nu % Ns, b = nu / Ns;
+    const double U = st.U;
+    double2 v = make_double2(0.0, 0.0);
+    if (mu == nu) {
+        if (i < st.nq) v.x += st.wq;
+        v = c_add(v, c_scale(c_mi(G[mu * n + mu]), U));
+        for (int g = 0; g < d.Nb; ++g)
+            if (g != a) {
+                int ig = i + g * Ns;
+                v = c_add(v, c_scale(c_mi(G[ig * n + ig]), 2.0 * U));
+            }
+        for (int m = 1; m <= d.nv; ++m) {
+            const double Vm = U * d.law[m - 1];
+            for (int dd = 0; dd < d.Nb; ++dd) {
+                if (i + m < Ns) {
+                    int p = (i + m) + dd * Ns;
+                    v = c_add(v, c_scale(c_mi(G[p * n + p]), 2.0 * Vm));
+                }
+                if (i - m >= 0) {
+                    int q = (i - m) + dd * Ns;
+                    v = c_add(v, c_scale(c_mi(G[q * n + q]), 2.0 * Vm));
+                }
+            }
+        }
+    } else {
+        if (a == b && abs(i - j) == 1) v.x += -d.t1;
+        if (i == j && abs(a - b) == 1) v.x += -d.t2;
+        if (i == j) v = c_add(v, c_scale(c_i(G[nu * n + mu]), U));
+        const int m = abs(i - j);
+        if (m >= 1 && m <= d.nv) v = c_add(v, c_scale(c_i(G[mu * n + nu]), U * d.law[m - 1]));
+    }
+    return v;
+}
+
+// Per (alpha, beta) pair, one warp: Psi factor Rt, Pi factors Q_xx / Q_xy and
+// the collision integral.  Block 0 also builds h.
+constexpr int kPrepWarps = 4;
+
+__global__ void __launch_bounds__(kPrepWarps * 32) k_prep(Dev d, int k)
+{
+    if (!*d.active) return;
+    const StageP st = d.cur->st[k];
+    const int n = d.n, Ns = d.Ns, Nb = d.Nb, nv = d.nv;
+    extern __shared__ double2 sm[];
+    double2 *sG = sm;  // n*n
+    const double2 *G1 = g1_stage(d, k);
+    for (int x = threadIdx.x; x < n * n; x += blockDim.x) sG[x] = G1[x];
+    __syncthreads();
+    if (blockIdx.x == 0)
+        for (int x = threadIdx.x; x < n * n; x += blockDim.x) d.h[x] = h_entry(d, sG, x / n, x % n, st);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double2 *wE = sm + n * n + warp * (4 * kMaxN);   // n entries
+    double2 *wDx = wE + kMaxN;                         // n
+    double2 *wDy = wDx + kMaxN;                        // n
+    double2 *wS = wDy + kMaxN;                         // R / S, Ns entries
+    const long long pair = (long long)blockIdx.x * kPrepWarps + warp;
+    if (pair >= (long long)n * n) return;
+    const int alpha = int(pair / n), beta = int(pair % n);
+    const double U = st.U;
+    if (!d.gate) {
+        if (lane == 0) d.Ix[pair] = make_double2(0.0, 0.0);
+        return;
+    }
+    // R[s] = sum_r G1[alpha][(s,r)] G1[(s,r)][beta]
+    for (int r = lane; r < n; r += 32) wE[r] = c_mul(sG[alpha * n + r], sG[r * n + beta]);
+    __syncwarp();
+    double2 Rv[2];
+    for (int q = 0; q < 2; ++q) {
+        int s = lane + 32 * q;
+        double2 acc = make_double2(0.0, 0.0);
+        if (s < Ns)
+            for (int b = 0; b < Nb; ++b) acc = c_add(acc, wE[s + b * Ns]);
+        Rv[q] = acc;
+    }
+    __syncwarp();
+    for (int q = 0; q < 2; ++q) {
+        int s = lane + 32 * q;
+        if (s < Ns) wS[s] = Rv[q];
+    }
+    __syncwarp();
+    for (int s = lane; s < Ns; s += 32) {
+        double2 acc = c_scale(wS[s], U);
+        for (int m = 1; m <= nv; ++m) {
+            const double Vm = U * d.law[m - 1];
+            double2 t = make_double2(0.0, 0.0);
+            if (s + m < Ns) t = c_add(t, wS[s + m]);
+            if (s - m >= 0) t = c_add(t, wS[s - m]);
+            acc = c_add(acc, c_scale(t, Vm));
+        }
+        d.Rt[pair * Ns + s] = acc;
+    }
+    __syncwarp();
+    // D -> S -> Vp -> Q
+    const double2 *Dx = d.D + pair * n, *Dy = d.D + d.n3 + pair * n;
+    for (int r = lane; r < n; r += 32) {
+        wDx[r] = Dx[r];
+        wDy[r] = Dy[r];
+    }
+    __syncwarp();
+    double2 Sv[2];
+    for (int q = 0; q < 2; ++q) {
+        int s = lane + 32 * q;
+        double2 acc = make_double2(0.0, 0.0);
+        if (s < Ns)
+            for (int b = 0; b < Nb; ++b) acc = c_add(acc, c_add(wDx[s + b * Ns], wDy[s + b * Ns]));
+        Sv[q] = acc;
+    }
+    __syncwarp();
+    for (int q = 0; q < 2; ++q) {
+        int s = lane + 32 * q;
+        if (s < Ns) wS[s] = Sv[q];
+    }
+    __syncwarp();
+    double2 *wVp = wE;  // reuse: Ns entries
+    for (int s = lane; s < Ns; s += 32) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int m = 1; m <= nv; ++m) {
+            const double Vm = U * d.law[m - 1];
+            double2 t = make_double2(0.0, 0.0);
+            if (s + m < Ns) t = c_add(t, wS[s + m]);
+            if (s - m >= 0) t = c_add(t, wS[s - m]);
+            acc = c_add(acc, c_scale(t, Vm));
+        }
+        wVp[s] = acc;
+    }
+    __syncwarp();
+    double2 *Qx = d.Q + pair * n, *Qy = d.Q + d.n3 + pair * n;
+    for (int r = lane; r < n; r += 32) {
+        const int s = r % Ns;
+        const double2 S = wS[s], vp = wVp[s];
+        double2 qx = c_mi(c_add(c_scale(c_sub(S, wDx[r]), U), vp));
+        double2 qy = c_mi(c_add(c_scale(c_sub(S, wDy[r]), U), vp));
+        Qx[r] = qx;
+        Qy[r] = qy;
+        if (r == alpha) d.Ix[pair] = qx;
+    }
+}
+
+// G1 side of a stage (commutators.h:28-51, G1_G2_t_step.h:24-47) and the
+// G1 RK bookkeeping (RK_solver.h:134-135, 204-208).  One block.
+__global__ void __launch_bounds__(1024) k_g1(Dev d, int k)
+{
+    if (!*d.active) return;
+    const StageP st = d.cur->st[k];
+    const int n = d.n;
+    extern __shared__ double2 sm[];
+    double2 *sH = sm, *sG = sm + n * n;
+    const double2 *G1 = g1_stage(d, k);
+    for (int x = threadIdx.x; x < n * n; x += blockDim.x) {
+        sH[x] = d.h[x];
+        sG[x] = G1[x];
+    }
+    __syncthreads();
+    double2 *G1n = g1_next(d, k);
+    for (int x = threadIdx.x; x < n * n; x += blockDim.x) {
+        const int mu = x / n, nu = x % n;
+        double2 hg = make_double2(0.0, 0.0), gh = make_double2(0.0, 0.0);
+        for (int r = 0; r < n; ++r) {
+            hg = c_mac(hg, sH[mu * n + r], sG[r * n + nu]);
+            gh = c_mac(gh, sG[mu * n + r], sH[r * n + nu]);
+        }
+        const double2 comm = c_sub(hg, gh);
+        const double2 K = c_mi(c_add(c_add(comm, d.Ix[x]), c_conj(d.Ix[nu * n + mu])));
+        if (d.debug) {
+            d.comm_dbg[x] = comm;
+            d.K1_dbg[x] = K;
+            continue;
+        }
+        const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : d.RK1[x], c_scale(K, st.w));
+        if (k < 3) {
+            d.RK1[x] = rk;
+            G1n[x] = c_add(d.Y1[x], c_scale(K, st.c_next));
+        } else {
+            d.Y1[x] = c_add(d.Y1[x], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
+        }
+    }
+}
+
+// Two-body commutator halves as Y = L X + X R on a batch of n x n matrices
+// held in shared memory ("natural" layout: row = slower index).
+//   CD = false: rows of M (particle indices), X_c[mu2][mu1] = G2[mu1 mu2; c],
+//               (L, R) = (h, h^T), result T = (H2 M) written to TAB.
+//   CD = true:  columns of M, X_r[nu2][nu1] = G2[r; nu1 nu2], (L, R) = (h^T, h),
+//               C = TAB - (M H2) then the fused epilogue: Psi, Pi, K2
+//               (G1_G2_t_step.h:55-86) and the RK4 bookkeeping
+//               (RK_solver.h:137-139, 209-213).
+// Each thread owns a 4 x 4 register tile with stride S = NP/4 in both
+// directions (conflict-free shared-memory rows).
+struct ApplyCfg {
+    int NP, LD, S, NB;
+};
+
+template <bool CD>
+__global__ void __launch_bounds__(256) k_apply(Dev d, int k, ApplyCfg cfg)
+{
+    if (!*d.active) return;
+    const int n = d.n, NP = cfg.NP, LD = cfg.LD, S = cfg.S, NB = cfg.NB;
+    const long long n2 = d.n2, n4 = d.n4;
+    const int t = blockIdx.y;
+    const long long m0 = (long long)blockIdx.x * NB;
+    const int nm = int(min((long long)NB, n2 - m0));
+    extern __shared__ double2 sm[];
+    double2 *Hs = sm, *HTs = sm + NP * LD, *Xs = sm + 2 * NP * LD;
+    double2 *Gs = Xs + (size_t)NB * NP * LD;  // CD only: n*n
+    const double2 *X = g2_stage(d, k) + t * n4;
+
+    for (int x = threadIdx.x; x < NP * NP; x += blockDim.x) {
+        const int r = x / NP, c = x % NP;
+        double2 v = (r < n && c < n) ? d.h[r * n + c] : make_double2(0.0, 0.0);
+        Hs[r * LD + c] = v;
+        HTs[c * LD + r] = v;
+    }
+    if (NP != n)
+        for (int x = threadIdx.x; x < NB * NP * LD; x += blockDim.x) Xs[x] = make_double2(0.0, 0.0);
+    if (CD) {
+        const double2 *G1 = g1_stage(d, k);
+        for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[x] = G1[x];
+    }
+    __syncthreads();
+    if (!CD) {
+        // (mu2, mu1, cb) with cb fastest: NB contiguous entries per row of M
+        for (long long e = threadIdx.x; e < n2 * NB; e += blockDim.x) {
+            const int cb = int(e % NB);
+            const long long p = e / NB;  // mu1 + n*mu2
+            const int mu1 = int(p % n), mu2 = int(p / n);
+            if (cb < nm) Xs[(size_t)cb * NP * LD + mu2 * LD + mu1] = X[p * n2 + m0 + cb];
+        }
+    } else {
+        for (long long e = threadIdx.x; e < (long long)nm * n2; e += blockDim.x) {
+            const int rb = int(e / n2);
+            const int c = int(e % n2);
+            const int nu1 = c % n, nu2 = c / n;
+            Xs[(size_t)rb * NP * LD + nu2 * LD + nu1] = X[(m0 + rb) * n2 + c];
+        }
+    }
+    __syncthreads();
+
+    const int mat = threadIdx.x / (S * S), tt = threadIdx.x % (S * S);
+    const int ti = tt / S, tj = tt % S;
+    const bool live = mat < nm;
+    double2 acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = make_double2(0.0, 0.0);
+    if (live) {
+        const double2 *L = CD ? HTs : Hs;
+        const double2 *R = CD ? Hs : HTs;
+        const double2 *Xm = Xs + (size_t)mat * NP * LD;
+        for (int r = 0; r < n; ++r) {
+            double2 l[4], xr[4], xc[4], rr[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                l[q] = L[(ti + S * q) * LD + r];
+                xc[q] = Xm[(ti + S * q) * LD + r];
+                xr[q] = Xm[r * LD + tj + S * q];
+                rr[q] = R[r * LD + tj + S * q];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    acc[a][b] = c_mac(acc[a][b], l[a], xr[b]);
+                    acc[a][b] = c_mac(acc[a][b], xc[a], rr[b]);
+                }
+        }
+    }
+
+    if (!CD) {
+        // stage through shared memory so the global stores run along cb
+        __syncthreads();
+        if (live) {
+            double2 *Ym = Xs + (size_t)mat * NP * LD;
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) Ym[(ti + S * a) * LD + tj + S * b] = acc[a][b];
+        }
+        __syncthreads();
+        double2 *T = d.TAB + t * n4;
+        for (long long e = threadIdx.x; e < n2 * NB; e += blockDim.x) {
+            const int cb = int(e % NB);
+            const long long p = e / NB;
+            const int mu1 = int(p % n), mu2 = int(p / n);
+            if (cb < nm) T[p * n2 + m0 + cb] = Xs[(size_t)cb * NP * LD + mu2 * LD + mu1];
+        }
+        return;
+    }
+
+    if (!live) return;
+    // ---- fused epilogue (CD) ----
+    const StageP st = d.cur->st[k];
+    const double U = st.U;
+    const int Ns = d.Ns;
+    const long long r = m0 + mat;
+    const int mu1 = int(r % n), mu2 = int(r / n);
+    const int si = mu1 % Ns, sj = mu2 % Ns;
+    const double2 *Tt = d.TAB + t * n4;
+    const double2 *Qt = d.Q + t * d.n3;
+    double2 *RKt = d.RK2 + t * n4;
+    double2 *Yt = d.Y2 + t * n4;
+    double2 *Dt = d.D + t * d.n3;
+    double2 *Nt = g2_next(d, k) + t * n4;
+    double2 *Kdbg = d.TMP0 + t * n4;
+    auto vdist = [&](int s1, int s2) -> double {
+        const int m = abs(s1 - s2);
+        return (m >= 1 && m <= d.nv) ? U * d.law[m - 1] : 0.0;
+    };
+    const double wij = U * double(si == sj) + vdist(si, sj);
+    const double2 *Rt1 = d.Rt + ((long long)mu1 * n) * Ns;  // + nu1*Ns + s
+    const double2 *Rt2 = d.Rt + ((long long)mu2 * n) * Ns;  // + nu2*Ns + s
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int nu2 = ti + S * a;
+        if (nu2 >= n) continue;
+        const int sl = nu2 % Ns;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int nu1 = tj + S * b;
+            if (nu1 >= n) continue;
+            const int sk = nu1 % Ns;
+            const long long x = r * n2 + nu1 + (long long)n * nu2;
+            const double2 C = c_sub(Tt[x], acc[a][b]);
+            const double2 g11 = Gs[mu1 * n + nu1], g22 = Gs[mu2 * n + nu2];
+            const double wd = wij - (U * double(sk == sl) + vdist(sk, sl));
+            double2 psi = c_scale(c_mul(g11, g22), wd);
+            psi = c_add(psi, c_i(c_mul(g22, c_sub(Rt1[nu1 * Ns + sj], Rt1[nu1 * Ns + sl]))));
+            psi = c_add(psi, c_i(c_mul(g11, c_sub(Rt2[nu2 * Ns + si], Rt2[nu2 * Ns + sk]))));
+            if (t == 0) {
+                psi = c_sub(psi, c_scale(c_mul(g11, g22), U * (double(mu1 == mu2) - double(nu1 == nu2))));
+                const double2 e1 = c_sub(c_mul(Gs[mu1 * n + mu2], Gs[mu2 * n + nu1]),
+                                         c_mul(Gs[mu1 * n + nu2], Gs[nu2 * n + nu1]));
+                const double2 e2 = c_sub(c_mul(Gs[mu2 * n + mu1], Gs[mu1 * n + nu2]),
+                                         c_mul(Gs[mu2 * n + nu1], Gs[nu1 * n + nu2]));
+                psi = c_add(psi, c_scale(c_mi(c_add(c_mul(g22, e1), c_mul(g11, e2))), U));
+            }
+            const long long q1 = ((long long)mu1 * n + nu1) * n, q2 = ((long long)nu2 * n + mu2) * n;
+            const double2 pi = c_mul(g22, c_sub(Qt[q1 + mu2], Qt[q1 + nu2]));
+            const double2 piP = c_mul(Gs[nu1 * n + mu1], c_sub(Qt[q2 + nu1], Qt[q2 + mu1]));
+            const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
+            if (d.debug) {
+                Kdbg[x] = K;
+                continue;
+            }
+            const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : RKt[x], c_scale(K, st.w));
+            if (k < 3) {
+                RKt[x] = rk;
+                const double2 tn = c_add(Yt[x], c_scale(K, st.c_next));
+                Nt[x] = tn;
+                if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = tn;
+            } else {
+                const double2 yn = c_add(Yt[x], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
+                Yt[x] = yn;
+                if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = yn;
+            }
+        }
+    }
+}
+
+// D[t][a][b][r] = Y2_t[a, r; b, r]
+__global__ void k_init_D(Dev d)
+{
+    const long long total = 2 * d.n3;
+    const int n = d.n;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const int t = int(e / d.n3);
+        const long long q = e % d.n3;
+        const int r = int(q % n), b = int((q / n) % n), a = int(q / d.n2);
+        d.D[e] = d.Y2[t * d.n4 + (long long)b + (long long)n * r + d.n2 * a + d.n2 * n * r];
+    }
+}
+
+// reference IDX_8D layout <-> device orbital layout
+__device__ __forceinline__ long long ref_index(int Ns, int Nb, long long x, int n)
+{
+    const int nu1 = int(x % n), nu2 = int((x / n) % n), mu1 = int((x / ((long long)n * n)) % n),
+              mu2 = int(x / ((long long)n * n * n));
+    const long long Ns2 = (long long)Ns * Ns, Nb2 = (long long)Nb * Nb;
+    const int k = nu1 % Ns, g = nu1 / Ns, l = nu2 % Ns, dd = nu2 / Ns;
+    const int i = mu1 % Ns, a = mu1 / Ns, j = mu2 % Ns, b = mu2 / Ns;
+    return (k + (long long)l * Ns) + (g + (long long)dd * Nb) * Ns2 + (i + (long long)j * Ns) * Ns2 * Nb2 +
+           (a + (long long)b * Nb) * Ns2 * Ns2 * Nb2;
+}
+
+__global__ void k_from_ref(const double2 *__restrict__ src, double2 *__restrict__ dst, int Ns, int Nb, long long n4)
+{
+    const int n = Ns * Nb;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n4; x += (long long)gridDim.x * blockDim.x)
+        dst[x] = src[ref_index(Ns, Nb, x, n)];
+}
+
+__global__ void k_to_ref(const double2 *__restrict__ src, double2 *__restrict__ dst, int Ns, int Nb, long long n4)
+{
+    const int n = Ns * Nb;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n4; x += (long long)gridDim.x * blockDim.x)
+        dst[ref_index(Ns, Nb, x, n)] = src[x];
+}
+
+}  // namespace g12

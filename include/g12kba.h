@@ -1,0 +1,150 @@
+/*
+ * g12kba - B200-native HF-GKBA G1-G2 propagation with GW self-energy.
+ *
+ * C ABI of libg12kba.so.  Plain pointers and sizes only.  Complex numbers are
+ * interleaved (re, im) doubles.  G1 is n x n row-major with orbital index
+ * mu = site + band*Ns (n = Ns*Nb).  G2 tensors handed across this boundary use
+ * the reference's flat layout IDX_8D(k,l,g,d,i,j,a,b) =
+ *   k + l*Ns + (g + d*Nb)*Ns^2 + (i + j*Ns)*Ns^2*Nb^2 + (a + b*Nb)*Ns^4*Nb^2
+ * (G12KBA-GW/src/headers/commutators.h:60), n^4 complex entries each.
+ *
+ * The reference (VlcekGroup/G12KBA) has no library API: its surface is the
+ * `input` file and the text outputs of G12KBA-GW/src/main/Main.cpp:44-62.  The
+ * seams these entry points replace are the free functions that Main.cpp calls;
+ * each declaration names the one it stands for.
+ *
+ * Conventions: the caller owns every host buffer, a context owns its device
+ * memory; one context per host thread; functions return G12_OK (0), a
+ * positive status (G12_GUARD_TRIPPED) or a negative error code, and never
+ * throw across the ABI.
+ */
+#ifndef G12KBA_H
+#define G12KBA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define G12_OK 0
+#define G12_GUARD_TRIPPED 1       /* RK_solver.h:106-110 density guard (outputs still valid) */
+#define G12_ERR_INVALID (-1)      /* bad argument or unsupported size */
+#define G12_ERR_CUDA (-2)         /* CUDA runtime failure; see g12_last_error */
+#define G12_ERR_NOMEM (-3)
+#define G12_ERR_PARSE (-4)        /* input value the reference's stod/stoi rejects */
+#define G12_ERR_NO_DEVICE (-5)    /* no CUDA device: there is no CPU fallback */
+
+#define G12_MAX_N 64              /* n = Ns*Nb supported by the kernels */
+
+enum g12_quench { G12_QUENCH_FULL = 0, G12_QUENCH_PULSE = 1 };
+enum g12_vlaw { G12_VLAW_EXP = 0, G12_VLAW_INV = 1 };
+enum g12_precision {
+    G12_PREC_FP64 = 0,    /* plain FP64 path (parity with the reference) */
+    G12_PREC_TF32X3 = 1,  /* two-body commutator on tcgen05 kind::tf32, 3-term split */
+    G12_PREC_BF16X3 = 2   /* two-body commutator on tcgen05 kind::f16 (bf16), 3-term split */
+};
+
+/* Run parameters: the globals of read_input.h:27-49 plus the extensions that
+ * the reference hard-codes (all defaults reproduce the reference). */
+typedef struct g12_params {
+    int32_t Ns, Nb, Nq;
+    int32_t time_steps;
+    int32_t HF, EHM;             /* booleans */
+    int32_t q_type;              /* g12_quench; input "none" gives FULL with qs=0, Nq=0 */
+    int32_t v_law;               /* g12_vlaw; EXP = U*exp(-0.7 r) as in AS.h:138 */
+    double t1, t2, t3, U, dt, quench_strength;
+    double AS_rate, AS_midpoint, quench_rate, quench_on_midpoint, quench_off_midpoint;
+    double quench_gate;          /* quench off while t < gate (RK_solver.h:141: 50) */
+    double as_dt;                /* AS step (AS.h:114-121: 0.1) */
+    double decay_rate;           /* EXP law rate (read_input.h:29: 0.7) */
+} g12_params;
+
+typedef struct g12_ctx g12_ctx;
+typedef struct g12_batch g12_batch;
+
+/* ---- host side: input, schedule, initial state, outputs ---------------- */
+
+/* read_input.h:29-49 defaults. */
+void g12_params_default(g12_params *p);
+
+/* read_input.h:53-146 (read_var_val + assign_vals): alternating key/value
+ * lines, first line containing the key as a substring.  The messages the
+ * reference prints go to `log` (may be NULL).  Extension keys: V_law (exp|inv),
+ * quench_gate, AS_dt. */
+int g12_read_input(const char *path, g12_params *p, char *log, int32_t logcap);
+
+/* AS.h:96-100 loop count and RK_solver.h:96,216 iteration count. */
+int64_t g12_as_steps(const g12_params *p);
+int64_t g12_rk_iterations(const g12_params *p);
+
+/* init_G.h:57-75 make_G0(..., p_number = Ns/2, U = 0): complex64 Hermitian
+ * eigen-solve of the hopping Hamiltonian, G1 = i * sum_{k<p} v_k v_k^H. */
+int g12_make_G0(const g12_params *p, int32_t p_number, double *G1_out);
+
+/* dipole.h:25-32 over T snapshots (host). */
+int g12_dipole(const double *traj, int64_t T, int32_t n, double *p_out);
+
+/* write_to_file.h:52-69 (real_/imag_<name>) and :26-34; std::ostream default
+ * formatting (6 significant digits). */
+int g12_write_cfile2D(const char *name, const double *traj, int64_t T, int32_t n2);
+int g12_write_rfile(const char *name, const double *data, int64_t count);
+
+/* ---- device context: one system ---------------------------------------- */
+
+int g12_create(const g12_params *p, int32_t precision, int32_t device, g12_ctx **out);
+int g12_destroy(g12_ctx *ctx);
+const char *g12_last_error(const g12_ctx *ctx);  /* NULL ctx: last creation error */
+
+/* State in/out (host buffers).  NULL G2 pointers on set mean zero; NULL on
+ * get skips that tensor.  set_state also resets the RK4 clock to t = 0. */
+int g12_set_state(g12_ctx *ctx, const double *G1, const double *G2xx, const double *G2xy);
+int g12_get_state(g12_ctx *ctx, double *G1, double *G2xx, double *G2xy);
+
+/* Adiabatic_switching (AS.h:63-214): all g12_as_steps() steps. */
+int g12_adiabatic_switch(g12_ctx *ctx, int64_t *steps_done);
+
+/* RK4 (RK_solver.h:64-226), continued from the context's clock: up to
+ * nsteps steps; traj_out (nullable) receives the snapshot of G1 taken at the
+ * start of each step (nsteps * n*n complex).  Returns G12_GUARD_TRIPPED when
+ * the site-0 density guard stops the run (*steps_done snapshots written, the
+ * last one the offending state). */
+int g12_propagate(g12_ctx *ctx, int64_t nsteps, double *traj_out, int64_t *steps_done);
+
+/* Same, with the trajectory left on the device: dipole_out (nullable, host)
+ * receives dipole.h:25-32 per snapshot, reduced on the GPU. */
+int g12_propagate_dipole(g12_ctx *ctx, int64_t nsteps, double *dipole_out, int64_t *steps_done);
+
+/* One right-hand-side evaluation on the given state (host buffers, G2 in the
+ * reference layout) with explicit stage scalars; returns the terms the
+ * reference computes in one RK stage (RK_solver.h:141-169):
+ *   h (HF.h:57), comm1 (commutators.h:28), Ix (collision_integral.h:27),
+ *   K1 (G1_G2_t_step.h:24), K2xx / K2xy (G1_G2_t_step.h:55, which combine
+ *   commutators.h:53, psi.h:26/157 and pi.h:25).
+ * V is U_eff * law(r) for r = 1..Ns-1 when EHM.  Any output may be NULL. */
+int g12_rhs(g12_ctx *ctx, const double *G1, const double *G2xx, const double *G2xy,
+            double U_eff, double w_quench, int32_t Nq_eff,
+            double *h, double *comm1, double *Ix, double *K1, double *K2xx, double *K2xy);
+
+/* Device time of the last g12_propagate* call's kernels (CUDA events, ms). */
+double g12_last_device_ms(const g12_ctx *ctx);
+
+/* Number of kernel launches one RK4 step issues (graph nodes). */
+int32_t g12_launches_per_step(const g12_ctx *ctx);
+
+/* Profiling: runs `nsteps` RK4 steps kernel by kernel (no graph) with CUDA
+ * events around every launch on the context's stream and returns the number
+ * of kernel kinds; avg_ms[i] (i < cap) receives kind i's mean launch time and
+ * calls_per_step[i] (nullable) its launches per step.  Advances the state. */
+int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms, int32_t *calls_per_step, int32_t cap);
+const char *g12_kernel_name(const g12_ctx *ctx, int32_t kind);
+
+/* Measured FP64 FMA throughput of `device` (TFLOP/s, 2 flops per FMA): the
+ * FP64 roofline denominator, which the tensor-core peaks do not cover. */
+double g12_fp64_peak_tflops(int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* G12KBA_H */

@@ -1,0 +1,48 @@
+#!/bin/bash
+# Oracle test infrastructure: builds the compiled-reference oracle into
+# oracle/_ref/ from the reference's own headers (G12KBA-GW/src/headers).
+#
+# The headers are copied to a temporary directory (never into this repository)
+# and patched there:
+#   P1 init_G.h:80      "\\Puts" -> "//Puts"   (stray backslash: compile error as shipped)
+#   P2 AS.h:72,138 and RK_solver.h:74
+#                       exp(-decay_rate*(i+1)) -> G12_VLAW(i+1)
+#                       (the harness picks the law: exp(-0.7 r), as shipped, or 1/(1+r))
+#   P3 RK_solver.h:80   "double t_temp;" -> "double t_temp = 0;" (read before set on step 0)
+#   P4 AS.h:78          "double U_AS;"   -> "double U_AS = NAN;" (read before set on step 0;
+#                       NAN keeps the first |U_AS-U|<=0 test false)
+# The G2/V/epsilon sizing defects are worked around in ref_harness.cpp on globals.
+# MKL is not installed: oracle/mkl_shim provides cblas_zgemm and LAPACKE_cheev.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REFROOT="${G12_REFERENCE:-/root/reference}"
+HDR="$REFROOT/G12KBA-GW/src/headers"
+OUT="$HERE/_ref"
+if [ ! -d "$HDR" ]; then
+    echo "build_ref: reference headers not found at $HDR" >&2
+    exit 1
+fi
+mkdir -p "$OUT"
+TMP="$(mktemp -d /tmp/g12ref.XXXXXX)"
+trap 'rm -rf "$TMP"' EXIT
+cp "$HDR"/*.h "$TMP"/
+
+sed -i 's#\\\\Puts#//Puts#' "$TMP/init_G.h"
+sed -i 's/exp(-decay_rate\*(i+1))/G12_VLAW(i+1)/g' "$TMP/AS.h" "$TMP/RK_solver.h"
+sed -i 's/^\(\s*\)double t_temp;/\1double t_temp = 0;/' "$TMP/RK_solver.h"
+sed -i 's/^\(\s*\)double U_AS;/\1double U_AS = NAN;/' "$TMP/AS.h"
+
+check() { if ! grep -q "$2" "$TMP/$1"; then echo "build_ref: patch '$2' missing in $1" >&2; exit 1; fi; }
+check init_G.h '//Puts'
+check AS.h 'U_AS\*G12_VLAW(i+1)'
+check RK_solver.h 'double t_temp = 0;'
+check AS.h 'double U_AS = NAN;'
+if grep -q '\\\\Puts' "$TMP/init_G.h"; then echo "build_ref: P1 not applied" >&2; exit 1; fi
+
+CXXFLAGS="-O3 -fopenmp -DNOTHREADS=1 -w"
+gcc -O3 -fPIC -c "$HERE/mkl_shim/mkl_shim.c" -I"$HERE/mkl_shim" -o "$TMP/mkl_shim.o"
+g++ $CXXFLAGS -DG12_REF_MAIN -I"$HERE/mkl_shim" -I"$TMP" "$HERE/ref_harness.cpp" "$TMP/mkl_shim.o" \
+    -o "$OUT/g12_ref" -lm
+g++ $CXXFLAGS -shared -fPIC -I"$HERE/mkl_shim" -I"$TMP" "$HERE/ref_harness.cpp" "$TMP/mkl_shim.o" \
+    -o "$OUT/libg12ref.so" -lm
+echo "build_ref: built $OUT/g12_ref and $OUT/libg12ref.so"

@@ -1,0 +1,115 @@
+"""Generates the golden vectors in tests/golden/ from the compiled reference.
+
+The reference (VlcekGroup/G12KBA) ships no tests or golden data, so these
+fixtures are outputs of its own routines, compiled from its headers by
+oracle/build_ref.sh (oracle/_ref/libg12ref.so for per-routine cases,
+oracle/_ref/g12_ref for full Main.cpp runs).  Inputs are seeded random
+complex arrays or the physics configurations listed below.
+
+Run from the repository root:  python tests/golden/make_golden.py
+"""
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import Config, Reference, run_reference_exe  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# (Ns, Nb) shapes for per-routine vectors: odd Ns, Nb = 1..3, Ns = 1 edge
+SHAPES = [(1, 2), (2, 1), (3, 1), (2, 2), (3, 2), (2, 3), (4, 2), (5, 1)]
+
+RUNS = {
+    # config-1 shape, shortened (BASELINE configs[0] with 200 of 2000 steps)
+    "run_c1_short": Config(Ns=4, Nb=1, Nq=2, time_steps=200, U=1.0, t1=1.0, t2=0.0, dt=0.02,
+                           AS_rate=0.5, AS_midpoint=10, q_type="full", quench_strength=1.0),
+    # extended model, Nb = 2, U/(1+r) law, pulse quench (masked by the t < 50 gate)
+    "run_ehm_nb2": Config(Ns=3, Nb=2, Nq=1, time_steps=60, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True,
+                          vlaw="inv", q_type="pulse", quench_strength=2.0, quench_rate=2,
+                          quench_on_midpoint=15, quench_off_midpoint=25, AS_rate=0.5, AS_midpoint=2),
+    # quench switched on at t >= 50: dt = 0.05, 1100 steps, exp law
+    "run_quench_on": Config(Ns=4, Nb=1, Nq=2, time_steps=1100, U=1.0, t1=1.0, dt=0.05, EHM=True,
+                            q_type="full", quench_strength=1.0, quench_rate=0.2, quench_on_midpoint=52,
+                            AS_rate=0.5, AS_midpoint=3),
+    # HF-only propagation (G2 frozen at zero, RK_solver.h:154)
+    "run_hf": Config(Ns=5, Nb=1, Nq=2, time_steps=300, U=1.5, t1=1.0, dt=0.02, HF=True,
+                     AS_rate=1.0, AS_midpoint=5),
+    # unstable step size: the site-0 density guard stops RK4 (RK_solver.h:101-110)
+    "run_guard": Config(Ns=2, Nb=1, Nq=1, time_steps=400, U=6.0, t1=1.0, dt=0.9,
+                        AS_rate=0.5, AS_midpoint=2),
+}
+
+
+def per_routine(ref):
+    rng = np.random.default_rng(20261203)
+    out = {}
+    for Ns, Nb in SHAPES:
+        n = Ns * Nb
+        tag = f"{Ns}x{Nb}"
+        G1 = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        G2a = rng.standard_normal(n ** 4) + 1j * rng.standard_normal(n ** 4)
+        G2b = rng.standard_normal(n ** 4) + 1j * rng.standard_normal(n ** 4)
+        V = rng.random(max(Ns - 1, 0))
+        U, t1, t2, w, Nq = 0.8, 1.0, 0.4, 0.3, min(2, Ns)
+        h = ref.h_hf(G1, Ns, Nb, U, t1, t2, w, V, Nq)
+        RK1 = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        RK2 = rng.standard_normal(n ** 4) + 1j * rng.standard_normal(n ** 4)
+        comm1 = ref.hG_comm(G1, h)
+        C2 = ref.h2_comm(G2a, h, Ns, Nb)
+        psi_xx = ref.psi(G1, Ns, Nb, U, V, 0)
+        psi_xy = ref.psi(G1, Ns, Nb, U, V, 1)
+        pi_ab = ref.pi(G1, G2a, G2b, U, Ns, Nb, V)
+        coll = ref.collision(G2a, G2b, Ns, Nb, U, V)
+        K1, RK1o = ref.G1_step(comm1, coll, RK1, 2.0, Ns, Nb)
+        K2, RK2o = ref.G2_step(C2, psi_xy, pi_ab, RK2, 2.0, Ns, Nb)
+        g0 = ref.make_G0(Ns, Nb, Ns // 2, t1, t2)
+        tr = rng.standard_normal((7, n, n)) + 1j * rng.standard_normal((7, n, n))
+        dip = ref.dipole(tr)
+        for k, v in dict(G1=G1, G2a=G2a, G2b=G2b, V=V, h=h, comm1=comm1, C2=C2, psi_xx=psi_xx,
+                         psi_xy=psi_xy, pi_ab=pi_ab, coll=coll, RK1=RK1, RK2=RK2, K1=K1, RK1o=RK1o,
+                         K2=K2, RK2o=RK2o, g0=g0, traj=tr, dipole=dip).items():
+            out[f"{tag}/{k}"] = v
+        out[f"{tag}/scalars"] = np.array([U, t1, t2, w, Nq], dtype=np.float64)
+    np.savez_compressed(os.path.join(OUT, "routines.npz"), **out)
+
+
+def full_runs():
+    for name, cfg in RUNS.items():
+        with tempfile.TemporaryDirectory() as d:
+            r = run_reference_exe(cfg, d)
+        traj = r["traj"]
+        keep = {
+            "g0": r["g0"], "g1_as": r["g1_as"], "g2xx_as": r["g2xx_as"], "g2xy_as": r["g2xy_as"],
+            "g2xx": r["g2xx"], "g2xy": r["g2xy"], "dipole": r["dipole"],
+            "T": np.array(traj.shape[0]),
+        }
+        if traj.shape[0] > 300:
+            keep["traj_every10"] = traj[::10]
+            keep["traj_last"] = traj[-1]
+        else:
+            keep["traj"] = traj
+        for k, v in cfg.__dict__.items():
+            keep["cfg_" + k] = np.array(v)
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **keep)
+        print(name, "T =", traj.shape[0], "max|G2| =", float(np.max(np.abs(r["g2xx"]))))
+
+
+def sample_input():
+    """The reference's only fixture (G12KBA-GW/input), kept verbatim as test
+    data for the input reader."""
+    src = os.path.join(os.environ.get("G12_REFERENCE", "/root/reference"), "G12KBA-GW", "input")
+    with open(src, "rb") as f, open(os.path.join(OUT, "sample_input"), "wb") as g:
+        g.write(f.read())
+
+
+if __name__ == "__main__":
+    if not Reference.available():
+        sys.exit("build the compiled reference first: oracle/build_ref.sh")
+    per_routine(Reference())
+    full_runs()
+    sample_input()

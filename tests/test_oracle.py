@@ -1,0 +1,106 @@
+"""The oracle (plain-C restatement, oracle/g12_oracle.c) pinned against the
+reference: committed golden vectors produced by the reference's own routines,
+and - where the compiled reference is present - fresh random cases."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import dipole_err, load_golden, rand_c, rel_err
+from oracle import Config, run_reference_exe
+
+SHAPES = [(1, 2), (2, 1), (3, 1), (2, 2), (3, 2), (2, 3), (4, 2), (5, 1)]
+TOL = 1e-13
+
+
+@pytest.mark.parametrize("Ns,Nb", SHAPES)
+def test_routines_vs_golden(oracle, Ns, Nb):
+    g = load_golden("routines.npz")
+    t = f"{Ns}x{Nb}/"
+    G1, G2a, G2b, V = g[t + "G1"], g[t + "G2a"], g[t + "G2b"], g[t + "V"]
+    U, t1, t2, w, Nq = g[t + "scalars"]
+    Nq = int(Nq)
+    h = oracle.h_hf(G1, Ns, Nb, U, t1, t2, w, V, Nq)
+    assert rel_err(h, g[t + "h"]) <= TOL
+    assert rel_err(oracle.hG_comm(G1, g[t + "h"]), g[t + "comm1"]) <= TOL
+    assert rel_err(oracle.h2_comm(G2a, g[t + "h"], Ns, Nb), g[t + "C2"]) <= TOL
+    assert rel_err(oracle.psi(G1, Ns, Nb, U, V, 0), g[t + "psi_xx"]) <= TOL
+    assert rel_err(oracle.psi(G1, Ns, Nb, U, V, 1), g[t + "psi_xy"]) <= TOL
+    assert rel_err(oracle.pi(G1, G2a, G2b, U, Ns, Nb, V), g[t + "pi_ab"]) <= TOL
+    assert rel_err(oracle.collision(G2a, G2b, Ns, Nb, U, V), g[t + "coll"]) <= TOL
+    K1, RK1 = oracle.G1_step(g[t + "comm1"], g[t + "coll"], g[t + "RK1"], 2.0, Ns, Nb)
+    assert rel_err(K1, g[t + "K1"]) <= TOL and rel_err(RK1, g[t + "RK1o"]) <= TOL
+    K2, RK2 = oracle.G2_step(g[t + "C2"], g[t + "psi_xy"], g[t + "pi_ab"], g[t + "RK2"], 2.0, Ns, Nb)
+    assert rel_err(K2, g[t + "K2"]) <= TOL and rel_err(RK2, g[t + "RK2o"]) <= TOL
+    # G0: same complex64 eigensolver contract -> bit-identical
+    assert np.array_equal(oracle.make_G0(Ns, Nb, Ns // 2, t1, t2), g[t + "g0"])
+    assert rel_err(oracle.dipole(g[t + "traj"]), g[t + "dipole"]) <= TOL
+
+
+def _cfg_from(g):
+    kw = {k[4:]: g[k].item() for k in g.files if k.startswith("cfg_")}
+    return Config(**kw)
+
+
+@pytest.mark.parametrize("name", ["run_c1_short", "run_ehm_nb2", "run_quench_on", "run_hf", "run_guard"])
+def test_full_runs_vs_golden(oracle, name):
+    g = load_golden(name + ".npz")
+    cfg = _cfg_from(g)
+    traj, G1, XX, XY = oracle.run(cfg, g["g0"])
+    T = int(g["T"])
+    assert traj.shape[0] == T
+    if "traj" in g.files:
+        ref = g["traj"]
+        if name == "run_guard":
+            # the guard trips on a NaN state: compare the finite prefix
+            ok = np.isfinite(ref).all(axis=(1, 2))
+            assert np.array_equal(np.isfinite(traj).all(axis=(1, 2)), ok)
+            assert rel_err(traj[ok], ref[ok]) <= 1e-12
+            return
+        assert rel_err(traj, ref) <= 1e-12
+    else:
+        assert rel_err(traj[::10], g["traj_every10"]) <= 1e-12
+        assert rel_err(traj[-1], g["traj_last"]) <= 1e-12
+    assert rel_err(XX, g["g2xx"], 1e-300) <= 1e-11
+    assert rel_err(XY, g["g2xy"], 1e-300) <= 1e-11
+    p = oracle.dipole(traj)
+    assert dipole_err(p, g["dipole"], traj) <= 1e-12
+
+
+def test_schedule_counts(oracle):
+    # AS.h:96-100 and RK_solver.h:96,216
+    c1 = Config(Ns=4, Nb=1, U=1.0, AS_rate=0.5, AS_midpoint=10, dt=0.02, time_steps=2000)
+    assert oracle.as_steps(c1) == 304
+    sample = Config(Ns=4, Nb=1, U=0.5, AS_rate=3, AS_midpoint=25, dt=0.07, time_steps=15000)
+    assert oracle.as_steps(sample) == 1373
+    assert oracle.rk_iterations(c1) == 2000
+    assert oracle.rk_iterations(Config(dt=0.01, time_steps=5000)) == 5001
+    assert oracle.rk_iterations(Config(dt=0.01, time_steps=10000)) == 10000
+    assert oracle.rk_iterations(Config(dt=0.01, time_steps=4000)) == 4000
+    assert oracle.rk_iterations(Config(dt=0.01, time_steps=6000)) == 6001
+
+
+def test_routines_vs_live_reference(oracle, reference):
+    rng = np.random.default_rng(7)
+    for Ns, Nb in [(3, 3), (6, 1), (4, 2)]:
+        n = Ns * Nb
+        G1, G2a, G2b = rand_c(rng, n, n), rand_c(rng, n ** 4), rand_c(rng, n ** 4)
+        V = rng.random(Ns - 1)
+        h = reference.h_hf(G1, Ns, Nb, 1.3, 1.0, 0.2, 0.5, V, 2)
+        assert rel_err(oracle.h_hf(G1, Ns, Nb, 1.3, 1.0, 0.2, 0.5, V, 2), h) <= TOL
+        assert rel_err(oracle.h2_comm(G2a, h, Ns, Nb), reference.h2_comm(G2a, h, Ns, Nb)) <= TOL
+        assert rel_err(oracle.psi(G1, Ns, Nb, 1.3, V, 1), reference.psi(G1, Ns, Nb, 1.3, V, 1)) <= TOL
+        assert rel_err(oracle.pi(G1, G2b, G2a, 1.3, Ns, Nb, V), reference.pi(G1, G2b, G2a, 1.3, Ns, Nb, V)) <= TOL
+        assert rel_err(oracle.collision(G2a, G2b, Ns, Nb, 1.3, V),
+                       reference.collision(G2a, G2b, Ns, Nb, 1.3, V)) <= TOL
+
+
+def test_full_run_vs_live_reference(oracle, reference):
+    cfg = Config(Ns=3, Nb=2, Nq=2, time_steps=40, U=1.2, t2=0.3, dt=0.02, EHM=True, vlaw="exp",
+                 AS_rate=0.4, AS_midpoint=1.5)
+    with tempfile.TemporaryDirectory() as d:
+        r = run_reference_exe(cfg, d)
+    traj, G1, XX, XY = oracle.run(cfg, r["g0"])
+    assert rel_err(traj, r["traj"]) <= 1e-12
+    assert rel_err(XY, r["g2xy"]) <= 1e-11
