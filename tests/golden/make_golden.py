@@ -39,8 +39,9 @@ RUNS = {
     # HF-only propagation (G2 frozen at zero, RK_solver.h:154)
     "run_hf": Config(Ns=5, Nb=1, Nq=2, time_steps=300, U=1.5, t1=1.0, dt=0.02, HF=True,
                      AS_rate=1.0, AS_midpoint=5),
-    # unstable step size: the site-0 density guard stops RK4 (RK_solver.h:101-110)
-    "run_guard": Config(Ns=2, Nb=1, Nq=1, time_steps=400, U=6.0, t1=1.0, dt=0.9,
+    # unstable step size: the site-0 density jumps past |2 Im G1_00| = 3 while
+    # still finite, and the guard stops RK4 (RK_solver.h:101-110)
+    "run_guard": Config(Ns=3, Nb=1, Nq=1, time_steps=200, U=4.0, t1=1.0, dt=0.35,
                         AS_rate=0.5, AS_midpoint=2),
 }
 

@@ -53,10 +53,9 @@ def test_full_runs_vs_golden(oracle, name):
     if "traj" in g.files:
         ref = g["traj"]
         if name == "run_guard":
-            # the guard trips on a NaN state: compare the finite prefix
-            ok = np.isfinite(ref).all(axis=(1, 2))
-            assert np.array_equal(np.isfinite(traj).all(axis=(1, 2)), ok)
-            assert rel_err(traj[ok], ref[ok]) <= 1e-12
+            # finite density excursion: the offending snapshot is the last one
+            assert rel_err(traj[:-1], ref[:-1]) <= 1e-12
+            assert abs(2 * traj[-1, 0, 0].imag) > 3 and abs(2 * ref[-1, 0, 0].imag) > 3
             return
         assert rel_err(traj, ref) <= 1e-12
     else:
