@@ -105,6 +105,9 @@ def lib():
         L.g12_kernel_name.argtypes = [C.c_void_p, C.c_int32]
         L.g12_fp64_peak_tflops.restype = C.c_double
         L.g12_fp64_peak_tflops.argtypes = [C.c_int32]
+        L.g12_rhs_noalloc.argtypes = [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                      C.c_double, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_char_p, C.c_int32]
         _lib = L
     return _lib
 

@@ -143,6 +143,26 @@ const char *g12_kernel_name(const g12_ctx *ctx, int32_t kind);
  * FP64 roofline denominator, which the tensor-core peaks do not cover. */
 double g12_fp64_peak_tflops(int32_t device);
 
+/* ---- allocation-free entry point ----------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code whose device memory is owned by another allocator (a caching or arena
+ * allocator that already reserved it) and latency-critical loops that cannot
+ * afford cudaMalloc's implicit synchronisation.  Computes what g12_rhs returns
+ * as K1, K2xx, K2xy, on caller-provided device buffers (G2 in the reference
+ * layout, interleaved complex128), enqueued on `stream` (NULL: the legacy
+ * default stream) on the current device.  All scratch lives in one static
+ * device array of about 6.4 MiB that every GPU loading the library holds until
+ * exit; n = Ns*Nb above G12_NOALLOC_MAX_N is rejected (G12_ERR_INVALID, message
+ * in `err`).  Calls share that array: calls whose GPU work overlaps race and
+ * must be serialised by the caller.  The first call on a device performs a
+ * one-time set-up (symbol address lookup, kernel attributes) and should come
+ * before any stream capture. */
+#define G12_NOALLOC_MAX_N 16
+int g12_rhs_noalloc(const g12_params *p, const double *G1_dev, const double *G2xx_dev,
+                    const double *G2xy_dev, double U_eff, double w_quench, int32_t Nq_eff,
+                    double *K1_dev, double *K2xx_dev, double *K2xy_dev, void *stream,
+                    char *err, int32_t errcap);
+
 #ifdef __cplusplus
 }
 #endif
