@@ -180,8 +180,10 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "bf16x3"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "bf16oz", "tf32x6", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-as", action="store_true",
+                    help="start the timed steps from G0 (profiling runs); the cost of a step does not depend on the state")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -198,7 +200,8 @@ def main():
     def prepared(prec):
         ctx = g12.Context(p, prec, local)
         ctx.set_state(G0)
-        ctx.adiabatic_switch()
+        if not args.skip_as:
+            ctx.adiabatic_switch()
         return ctx
 
     ctx = prepared(args.precision)

@@ -272,6 +272,13 @@ int run_steps(g12_ctx *ctx, long long steps, double *traj_out, double *dip_out, 
             if (dip_out && got > 0)
                 CK(cudaMemcpy(dip_out + base, ctx->d.dip + off, got * sizeof(double), cudaMemcpyDeviceToHost));
         }
+        if (ctx->prec != G12_PREC_FP64) {
+            const int me = mixed_error(ctx->mixed);
+            if (me) {
+                ctx->err = "tensor-core pipeline wait expired (code " + std::to_string(me) + ")";
+                return G12_ERR_CUDA;
+            }
+        }
         base += got;
         if (status > 0) {
             *done = base;
@@ -296,7 +303,7 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
         g_create_error = "unsupported size: need 1 <= Ns*Nb <= 64";
         return G12_ERR_INVALID;
     }
-    if (precision < G12_PREC_FP64 || precision > G12_PREC_BF16X3) {
+    if (precision < G12_PREC_FP64 || precision > G12_PREC_TF32X6) {
         g_create_error = "unknown precision mode";
         return G12_ERR_INVALID;
     }
@@ -462,6 +469,12 @@ extern "C" int g12_get_state(g12_ctx *ctx, double *G1, double *G2xx, double *G2x
     if (!ctx) return G12_ERR_INVALID;
     CK(cudaSetDevice(ctx->device));
     if (G1) CK(cudaMemcpyAsync(G1, ctx->d.Y1, ctx->n2 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->s));
+    if (ctx->prec != G12_PREC_FP64 && (G2xx || G2xy)) {
+        if (mixed_to_full(ctx->mixed, ctx->d, ctx->s)) {
+            ctx->err = "state expansion failed";
+            return G12_ERR_CUDA;
+        }
+    }
     int rc = download_g2(ctx, ctx->d.Y2, G2xx);
     if (!rc) {
         CK(cudaStreamSynchronize(ctx->s));
@@ -564,15 +577,18 @@ extern "C" int g12_rhs(g12_ctx *ctx, const double *G1, const double *G2xx, const
     if (Ix) CK(cudaMemcpyAsync(Ix, dd.Ix, b2, cudaMemcpyDeviceToHost, ctx->s));
     if (K1) CK(cudaMemcpyAsync(K1, dd.K1_dbg, b2, cudaMemcpyDeviceToHost, ctx->s));
     CK(cudaStreamSynchronize(ctx->s));
-    rc = download_g2(ctx, dd.TMP0, K2xx);
+    // FP64: K2 in TMP0; symmetric engine: K2 in Y2 (its full-state staging buffer)
+    double2 *K2src = (ctx->prec == G12_PREC_FP64) ? dd.TMP0 : dd.Y2;
+    rc = download_g2(ctx, K2src, K2xx);
     if (!rc) {
         CK(cudaStreamSynchronize(ctx->s));
-        rc = download_g2(ctx, dd.TMP0 + ctx->n4, K2xy);
+        rc = download_g2(ctx, K2src + ctx->n4, K2xy);
     }
     CK(cudaStreamSynchronize(ctx->s));
-    // the debug pass replaced the state's D; rebuild it from Y2
-    k_init_D<<<592, 256, 0, ctx->s>>>(ctx->d);
-    CK(cudaStreamSynchronize(ctx->s));
+    if (ctx->prec != G12_PREC_FP64 && mixed_error(ctx->mixed)) {
+        ctx->err = "tensor-core pipeline wait expired";
+        return G12_ERR_CUDA;
+    }
     return rc;
 }
 

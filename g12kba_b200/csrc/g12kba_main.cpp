@@ -4,8 +4,8 @@
 // imag_G1.txt, dipole.txt and progress.txt in the working directory with the
 // reference's formats and stdout lines.
 //
-// Extension input keys (ignored by the reference): precision (fp64 | tf32x3 |
-// bf16x3), device, G0_file (n*n complex128 binary replacing make_G0), plus
+// Extension input keys (ignored by the reference): precision (fp64 | bf16oz |
+// tf32x3 | tf32x6 | fp32), device, G0_file (n*n complex128 binary replacing make_G0), plus
 // V_law, quench_gate and AS_dt handled by g12_read_input.
 #include "g12kba.h"
 
@@ -45,7 +45,9 @@ int main(int argc, char **argv)
     int prec = G12_PREC_FP64;
     std::string pv = ext_value("precision");
     if (pv == "tf32x3") prec = G12_PREC_TF32X3;
-    else if (pv == "bf16x3") prec = G12_PREC_BF16X3;
+    else if (pv == "tf32x6") prec = G12_PREC_TF32X6;
+    else if (pv == "bf16oz") prec = G12_PREC_BF16OZ;
+    else if (pv == "fp32") prec = G12_PREC_FP32;
     int device = 0;
     std::string dv = ext_value("device");
     if (!dv.empty()) device = std::atoi(dv.c_str());

@@ -1,0 +1,331 @@
+// Mixed-precision ("symmetric") engine kernels.
+//
+// Physical states of the reference's propagation obey two exact symmetries of
+// G2[mu1 mu2; nu1 nu2] (they hold to round-off in the reference's own output,
+// starting from G2 = 0):
+//   exchange  e:  G2[mu2 mu1; nu2 nu1] = G2[mu1 mu2; nu1 nu2]
+//   Hermitian Pe: G2[nu1 nu2; mu1 mu2] = conj(G2[mu1 mu2; nu1 nu2])
+// i.e. M = G2 as an n^2 x n^2 matrix (rows r = mu1 + n*mu2, columns
+// c = nu1 + n*nu2) is Hermitian and exchange-symmetric, and h is Hermitian.
+// Then the two-body commutator of commutators.h:53-99 needs one contraction:
+//   T1 = (h (x) 1) M,   W = H2 M = T1 + e(T1),   C = H2 M - M H2 = W - W^H.
+// k_sym_gemm* computes W per tile of rows {all mu2} x {c, cbar} (closed under
+// e), k_sym_epi forms C = W - W^H on pairs of 32 x 32 tiles (R, C) / (C, R) and
+// fuses the rest of the stage (Psi, Pi, K2, RK4 bookkeeping) like k_apply<true>.
+//
+// Storage (per tensor t = xx, xy):
+//   TMP  (FP32, GEMM input):  ((mu2*n^2 + c)*2 + part)*n + mu1
+//   W    (FP32):              (c*2 + part)*n^2 + r
+//   Yc, Ac (FP64 complex):    Hermitian-compressed state and RK4 sum: for each
+//                             tile pair p = (Rb <= Cb) of 32 x 32 blocks,
+//                             [p][c_local*32 + r_local].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fp64_kernels.cuh"
+
+namespace g12 {
+
+constexpr int kTB = 32;  // epilogue tile edge (rows r and columns c of M)
+
+struct SymDev {
+    Dev d;                  // G1 side, tables (Q, Rt, D), schedule, snapshot ring
+    int n, cpt;             // cpt: c values per GEMM tile (= 128 / n)
+    int gemm_tiles;         // GEMM tiles per tensor
+    int nblk, npairs;       // epilogue blocks per edge, tile pairs per tensor
+    long long n4;
+    float *TMPa, *TMPb;     // 2 tensors each
+    float *W;               // 2 tensors
+    double2 *Yc, *Ac;       // 2 tensors x npairs x kTB^2
+    double2 *Qt, *Rtt;      // transposed copies of Q ([r][b][a]) and Rt ([s][b][a])
+    const int *gemm_c;      // [gemm_tiles][cpt] c values
+    const int *gemm_partner;// [gemm_tiles][cpt] slot of cbar in the same tile
+    const int2 *pairs;      // [npairs] (Rb, Cb), Rb <= Cb
+    int *err;               // device error word (bounded waits)
+};
+
+// stage k reads TMPb (k even) or TMPa (k odd) and writes the other one
+__device__ __forceinline__ const float *sym_in(const SymDev &s, int k) { return (k & 1) ? s.TMPa : s.TMPb; }
+__device__ __forceinline__ float *sym_out(const SymDev &s, int k) { return (k & 1) ? s.TMPb : s.TMPa; }
+
+__device__ __forceinline__ long long tmp_index(int n, int mu1, int mu2, int c, int part)
+{
+    return (((long long)mu2 * n * n + c) * 2 + part) * n + mu1;
+}
+
+// Transposed table copies for coalesced epilogue reads: Qt[t][r][b][a] = Q[t][a][b][r],
+// Rtt[s][b][a] = Rt[a][b][s].  One thread per element.
+__global__ void k_sym_tables(SymDev s)
+{
+    if (!*s.d.active || !s.d.gate) return;
+    const int n = s.n, Ns = s.d.Ns;
+    const long long n3 = (long long)n * n * n;
+    const long long tot = 2 * n3 + (long long)n * n * Ns;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        if (e < 2 * n3) {
+            const int t = int(e / n3);
+            const long long q = e % n3;  // output index: (r*n + b)*n + a
+            const int a = int(q % n), b = int((q / n) % n), r = int(q / ((long long)n * n));
+            s.Qt[t * n3 + q] = s.d.Q[t * n3 + ((long long)a * n + b) * n + r];
+        } else {
+            const long long q = e - 2 * n3;  // (s*n + b)*n + a
+            const int a = int(q % n), b = int((q / n) % n), sidx = int(q / ((long long)n * n));
+            s.Rtt[q] = s.d.Rt[((long long)a * n + b) * Ns + sidx];
+        }
+    }
+}
+
+// Reference FP32 SIMT version of the W contraction (same tiles as the
+// tensor-core kernel): T1[mu1][mu2][c] = sum_rho h[mu1][rho] X[rho][mu2][c].
+__global__ void __launch_bounds__(256) k_sym_gemm_simt(SymDev s, int k)
+{
+    if (!*s.d.active) return;
+    const int n = s.n, cpt = s.cpt, rows = cpt * n;
+    extern __shared__ float smf[];
+    float *X = smf;                         // [rows][2n]
+    float *S = X + rows * 2 * n;            // [rows][2n + 1] (T1 staging)
+    float2 *H = reinterpret_cast<float2 *>(S + rows * (2 * n + 1));  // [n][n]
+    const int t = blockIdx.x / s.gemm_tiles, g = blockIdx.x % s.gemm_tiles;
+    const float *Xg = sym_in(s, k) + t * 2 * s.n4;
+    for (int x = threadIdx.x; x < n * n; x += blockDim.x)
+        H[x] = make_float2(float(s.d.h[x].x), float(s.d.h[x].y));
+    for (int e = threadIdx.x; e < rows * 2 * n; e += blockDim.x) {
+        const int row = e / (2 * n), kk = e % (2 * n);
+        const int slot = row / n, mu2 = row % n;
+        const int c = s.gemm_c[g * cpt + slot];
+        X[e] = Xg[((long long)mu2 * n * n + c) * 2 * n + kk];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
+        const int row = e / n, mu1 = e % n;
+        float re = 0.f, im = 0.f;
+        const float *xr = X + row * 2 * n;
+        for (int r = 0; r < n; ++r) {
+            const float2 hv = H[mu1 * n + r];
+            const float gr = xr[r], gi = xr[n + r];
+            re = fmaf(hv.x, gr, re);
+            re = fmaf(-hv.y, gi, re);
+            im = fmaf(hv.x, gi, im);
+            im = fmaf(hv.y, gr, im);
+        }
+        S[row * (2 * n + 1) + mu1] = re;
+        S[row * (2 * n + 1) + n + mu1] = im;
+    }
+    __syncthreads();
+    // W[mu1][mu2][c] = T1[mu1][mu2][c] + T1[mu2][mu1][cbar]
+    float *Wg = s.W + t * 2 * s.n4;
+    const long long n2 = (long long)n * n;
+    for (int e = threadIdx.x; e < cpt * 2 * n * n; e += blockDim.x) {
+        const int r = e % (n * n), part = (e / (n * n)) % 2, slot = e / (2 * n * n);
+        const int mu1 = r % n, mu2 = r / n;
+        const int ps = s.gemm_partner[g * cpt + slot];
+        const float v = S[(slot * n + mu2) * (2 * n + 1) + part * n + mu1] +
+                        S[(ps * n + mu1) * (2 * n + 1) + part * n + mu2];
+        const int c = s.gemm_c[g * cpt + slot];
+        Wg[((long long)c * 2 + part) * n2 + r] = v;
+    }
+}
+
+// Stage epilogue on a tile pair (R, C) / (C, R): C = W - W^H, Psi, Pi, K2,
+// RK4 bookkeeping on the compressed state, next-stage input (both tiles, FP32),
+// particle-2 diagonal D (FP64).
+__global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
+{
+    if (!*s.d.active) return;
+    const Dev &d = s.d;
+    const int n = s.n, Ns = d.Ns;
+    const long long n2 = (long long)n * n, n3 = n2 * n;
+    const int t = blockIdx.y;
+    const int p = blockIdx.x;
+    const int2 rc = s.pairs[p];
+    const int R0 = rc.x * kTB, C0 = rc.y * kTB;
+    const bool diag = rc.x == rc.y;
+    extern __shared__ double2 smd[];
+    double2 *Gs = smd;                                 // n*n
+    float2 *Wrc = reinterpret_cast<float2 *>(Gs + n * n);  // [c_l][r_l] = W[R0+r_l][C0+c_l]
+    float2 *Wcr = Wrc + kTB * (kTB + 1);               // [r_l][c_l] = W[C0+c_l][R0+r_l]
+    double2 *Ks = reinterpret_cast<double2 *>(Wcr + kTB * (kTB + 1));  // [c_l][r_l] tmp_next (or K)
+    const float *Wg = s.W + t * 2 * s.n4;
+    const double2 *G1 = (k & 1) ? d.G1t1 : d.G1t0;
+    for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[x] = G1[x];
+    for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+        const int rl = e % kTB, cl = e / kTB;
+        // W[R0+rl][C0+cl] at (c*2+part)*n2 + r: contiguous in rl
+        const long long b1 = (long long)(C0 + cl) * 2 * n2 + R0 + rl;
+        Wrc[cl * (kTB + 1) + rl] = make_float2(Wg[b1], Wg[b1 + n2]);
+        // W[C0+rl'][R0+cl'] with rl' = rl as the row offset inside block C
+        const long long b2 = (long long)(R0 + cl) * 2 * n2 + C0 + rl;
+        Wcr[cl * (kTB + 1) + rl] = make_float2(Wg[b2], Wg[b2 + n2]);
+    }
+    __syncthreads();
+
+    const StageP st = d.cur->st[k];
+    const double U = st.U;
+    const double2 *Qo = d.Q + t * n3, *Qt = s.Qt + t * n3;
+    double2 *Yc = s.Yc + ((long long)t * s.npairs + p) * kTB * kTB;
+    double2 *Ac = s.Ac + ((long long)t * s.npairs + p) * kTB * kTB;
+    auto vdist = [&](int s1, int s2) -> double {
+        const int m = abs(s1 - s2);
+        return (m >= 1 && m <= d.nv) ? U * d.law[m - 1] : 0.0;
+    };
+    for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+        const int rl = e % kTB, cl = e / kTB;
+        const int r = R0 + rl, c = C0 + cl;
+        const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
+        const float2 w1 = Wrc[cl * (kTB + 1) + rl];
+        // W[c][r] = Wcr at (row offset cl in block C -> index rl' = cl, col r -> cl' = rl)
+        const float2 w2 = Wcr[rl * (kTB + 1) + cl];
+        const double2 C = make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
+        const int si = mu1 % Ns, sj = mu2 % Ns, sk = nu1 % Ns, sl = nu2 % Ns;
+        const double2 g11 = Gs[mu1 * n + nu1], g22 = Gs[mu2 * n + nu2];
+        const double wd = (U * double(si == sj) + vdist(si, sj)) - (U * double(sk == sl) + vdist(sk, sl));
+        double2 psi = c_scale(c_mul(g11, g22), wd);
+        const double2 *Rtt = s.Rtt;
+        psi = c_add(psi, c_i(c_mul(g22, c_sub(Rtt[((long long)sj * n + nu1) * n + mu1], Rtt[((long long)sl * n + nu1) * n + mu1]))));
+        const double2 *Rt2 = d.Rt + ((long long)mu2 * n + nu2) * Ns;
+        psi = c_add(psi, c_i(c_mul(g11, c_sub(Rt2[si], Rt2[sk]))));
+        if (t == 0) {
+            psi = c_sub(psi, c_scale(c_mul(g11, g22), U * (double(mu1 == mu2) - double(nu1 == nu2))));
+            const double2 e1 = c_sub(c_mul(Gs[mu1 * n + mu2], Gs[mu2 * n + nu1]), c_mul(Gs[mu1 * n + nu2], Gs[nu2 * n + nu1]));
+            const double2 e2 = c_sub(c_mul(Gs[mu2 * n + mu1], Gs[mu1 * n + nu2]), c_mul(Gs[mu2 * n + nu1], Gs[nu1 * n + nu2]));
+            psi = c_add(psi, c_scale(c_mi(c_add(c_mul(g22, e1), c_mul(g11, e2))), U));
+        }
+        // Pi[x] = G1[mu2][nu2] (Q[mu1][nu1][mu2] - Q[mu1][nu1][nu2]); Qt[r][b][a] = Q[a][b][r]
+        const double2 pi = c_mul(g22, c_sub(Qt[((long long)mu2 * n + nu1) * n + mu1], Qt[((long long)nu2 * n + nu1) * n + mu1]));
+        const long long q2 = ((long long)nu2 * n + mu2) * n;
+        const double2 piP = c_mul(Gs[nu1 * n + mu1], c_sub(Qo[q2 + nu1], Qo[q2 + mu1]));
+        const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
+        Ks[cl * kTB + rl] = K;
+    }
+    __syncthreads();
+    if (diag) {
+        // keep the diagonal block exactly Hermitian: K <- (K + K^H) / 2
+        double2 sym[4];
+        int cnt = 0;
+        for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+            const int rl = e % kTB, cl = e / kTB;
+            const double2 a = Ks[cl * kTB + rl], b = c_conj(Ks[rl * kTB + cl]);
+            sym[cnt++] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
+        }
+        __syncthreads();
+        cnt = 0;
+        for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+            const int rl = e % kTB, cl = e / kTB;
+            Ks[cl * kTB + rl] = sym[cnt++];
+        }
+        __syncthreads();
+    }
+    if (d.debug) {
+        // K of both tiles into d.Y2 in the device orbital layout x = c + n^2 r
+        double2 *Kd = d.Y2 + t * n2 * n2;
+        for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+            const int rl = e % kTB, cl = e / kTB;
+            const double2 K = Ks[cl * kTB + rl];
+            Kd[(long long)(R0 + rl) * n2 + C0 + cl] = K;
+            Kd[(long long)(C0 + cl) * n2 + R0 + rl] = c_conj(K);
+        }
+        return;
+    }
+    // RK4 bookkeeping on the compressed state; next-stage input value in Ks
+    double2 *Dt = d.D + t * n3;
+    for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+        const int rl = e % kTB, cl = e / kTB;
+        const double2 K = Ks[cl * kTB + rl];
+        const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : Ac[e], c_scale(K, st.w));
+        double2 v;
+        if (k < 3) {
+            Ac[e] = rk;
+            v = c_add(Yc[e], c_scale(K, st.c_next));
+        } else {
+            v = c_add(Yc[e], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
+            Yc[e] = v;
+        }
+        Ks[cl * kTB + rl] = v;
+        const int r = R0 + rl, c = C0 + cl;
+        const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
+        if (mu2 == nu2) {
+            Dt[((long long)mu1 * n + nu1) * n + mu2] = v;
+            // the mirrored element (nu1, nu2; mu1, mu2) holds conj(v)
+            if (!diag) Dt[((long long)nu1 * n + mu1) * n + nu2] = c_conj(v);
+        }
+    }
+    __syncthreads();
+    float *Out = sym_out(s, k) + t * 2 * s.n4;
+    // tile (R, C): fastest index mu1 = r % n follows rl
+    for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+        const int rl = e % kTB, cl = e / kTB;
+        const int r = R0 + rl, c = C0 + cl;
+        const double2 v = Ks[cl * kTB + rl];
+        const long long o = tmp_index(n, r % n, r / n, c, 0);
+        Out[o] = float(v.x);
+        Out[o + n] = float(v.y);
+    }
+    if (!diag) {
+        // tile (C, R): element (c, r) = conj(v); fastest index nu1 = c % n follows cl
+        for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+            const int cl = e % kTB, rl = e / kTB;
+            const int r = R0 + rl, c = C0 + cl;
+            const double2 v = Ks[cl * kTB + rl];
+            const long long o = tmp_index(n, c % n, c / n, r, 0);
+            Out[o] = float(v.x);
+            Out[o + n] = float(-v.y);
+        }
+    }
+}
+
+// Full FP64 state (device orbital layout, Y2 of the general engine) -> Yc,
+// TMPb (stage-0 input) and D.  One block per tile pair and tensor.
+__global__ void k_sym_pack(SymDev s, const double2 *Yfull)
+{
+    const int n = s.n;
+    const long long n2 = (long long)n * n, n3 = n2 * n;
+    const int t = blockIdx.y, p = blockIdx.x;
+    const int2 rc = s.pairs[p];
+    const int R0 = rc.x * kTB, C0 = rc.y * kTB;
+    const double2 *Y = Yfull + t * s.n4;
+    double2 *Yc = s.Yc + ((long long)t * s.npairs + p) * kTB * kTB;
+    float *Out = s.TMPb + t * 2 * s.n4;
+    double2 *Dt = s.d.D + t * n3;
+    for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+        const int rl = e % kTB, cl = e / kTB;
+        const int r = R0 + rl, c = C0 + cl;
+        const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
+        // device orbital layout: x = nu1 + n*nu2 + n^2*mu1 + n^3*mu2
+        const double2 v = Y[(long long)c + n2 * mu1 + n3 * mu2];
+        Yc[e] = v;
+        long long o = tmp_index(n, mu1, mu2, c, 0);
+        Out[o] = float(v.x);
+        Out[o + n] = float(v.y);
+        if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = v;
+        if (rc.x != rc.y) {
+            o = tmp_index(n, nu1, nu2, r, 0);
+            Out[o] = float(v.x);
+            Out[o + n] = float(-v.y);
+            if (nu2 == mu2) Dt[((long long)nu1 * n + mu1) * n + nu2] = c_conj(v);
+        }
+    }
+}
+
+// Yc -> full FP64 state in the device orbital layout (Hermitian expansion).
+__global__ void k_sym_unpack(SymDev s, double2 *Yfull)
+{
+    const int n = s.n;
+    const long long n2 = (long long)n * n, n3 = n2 * n;
+    const int t = blockIdx.y, p = blockIdx.x;
+    const int2 rc = s.pairs[p];
+    const int R0 = rc.x * kTB, C0 = rc.y * kTB;
+    double2 *Y = Yfull + t * s.n4;
+    const double2 *Yc = s.Yc + ((long long)t * s.npairs + p) * kTB * kTB;
+    for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+        const int rl = e % kTB, cl = e / kTB;
+        const int r = R0 + rl, c = C0 + cl;
+        const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
+        const double2 v = Yc[e];
+        Y[(long long)c + n2 * mu1 + n3 * mu2] = v;
+        if (rc.x != rc.y) Y[(long long)r + n2 * nu1 + n3 * nu2] = c_conj(v);
+    }
+}
+
+}  // namespace g12

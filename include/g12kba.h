@@ -41,9 +41,21 @@ enum g12_quench { G12_QUENCH_FULL = 0, G12_QUENCH_PULSE = 1 };
 enum g12_vlaw { G12_VLAW_EXP = 0, G12_VLAW_INV = 1 };
 enum g12_precision {
     G12_PREC_FP64 = 0,    /* plain FP64 path (parity with the reference) */
-    G12_PREC_TF32X3 = 1,  /* two-body commutator on tcgen05 kind::tf32, 3-term split */
-    G12_PREC_BF16X3 = 2   /* two-body commutator on tcgen05 kind::f16 (bf16), 3-term split */
+    G12_PREC_TF32X3 = 1,  /* two-body commutator on tcgen05 kind::tf32: 2 tf32 pieces, 3 products */
+    G12_PREC_BF16OZ = 2,  /* tcgen05 kind::f16: exact 7-bit integer digits in bf16 (4 per operand,
+                             10 products), unbiased; the accurate mixed mode */
+    G12_PREC_FP32 = 3,    /* symmetric engine with an FP32 CUDA-core contraction (checker) */
+    G12_PREC_TF32X6 = 4   /* tcgen05 kind::tf32: 3 tf32 pieces per operand, 6 products */
 };
+/* The mixed modes (TF32X3, TF32X6, FP32) use the symmetric engine: they
+ * require the physical G2 symmetries G2[mu2 mu1; nu2 nu1] = G2[mu1 mu2; nu1 nu2]
+ * and G2[nu1 nu2; mu1 mu2] = conj(G2[mu1 mu2; nu1 nu2]) (every state reached
+ * from G2 = 0 has them; set_state keeps the upper 32 x 32 blocks of G2 seen as
+ * an n^2 x n^2 matrix) and keep the RK4 state in FP64.  n = Ns*Nb must be 16 or
+ * 32 for the tensor-core modes and 8, 16, 32 or 64 for FP32.  TF32X3/TF32X6
+ * inherit the tensor cores' biased FP32 accumulation (about -4e-8 relative per
+ * contraction on B200), which accumulates into a linear phase drift of G1;
+ * BF16OZ keeps every partial sum an exact integer and has no such bias. */
 
 /* Run parameters: the globals of read_input.h:27-49 plus the extensions that
  * the reference hard-codes (all defaults reproduce the reference). */

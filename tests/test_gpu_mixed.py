@@ -1,0 +1,85 @@
+"""Mixed-precision (symmetric) engine: right-hand side against the oracle on
+states with the physical G2 symmetries, and propagation against the FP64 path.
+Bars: RHS terms 2e-5 relative (FP32 intermediates); G1 trajectories 1e-6
+relative to max |G1| against FP64 (the metric's error budget)."""
+import numpy as np
+import pytest
+
+from conftest import rand_c, rel_err
+from oracle import Config, idx8_to_orbital
+from test_gpu_parity import oracle_rhs, params_of
+
+pytestmark = pytest.mark.gpu
+
+MIXED_RHS_TOL = 2e-5
+TRAJ_TOL = 1e-6
+
+
+def physical_state(rng, Ns, Nb, scale=1e-2):
+    """Random G1 = i*rho (rho Hermitian) and G2 tensors with the exchange and
+    Hermitian symmetries, in the reference layout."""
+    n = Ns * Nb
+    a = rand_c(rng, n, n)
+    G1 = 1j * (a + a.conj().T) / 4
+    perm = idx8_to_orbital(Ns, Nb)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(perm.size)
+    out = []
+    for _ in range(2):
+        X = (scale * rand_c(rng, n ** 4)).reshape(n, n, n, n)  # axes [mu2][mu1][nu2][nu1]
+        S = (X + X.transpose(1, 0, 3, 2) + np.conj(X.transpose(2, 3, 0, 1)) + np.conj(X.transpose(3, 2, 1, 0))) / 4
+        out.append(S.reshape(-1)[inv])
+    return G1, out[0], out[1]
+
+
+@pytest.mark.parametrize("prec", ["fp32", "tf32x3", "bf16oz"])
+@pytest.mark.parametrize("Ns,Nb", [(8, 2), (16, 2), (16, 1), (4, 2)])
+def test_mixed_rhs_vs_oracle(g12, oracle, prec, Ns, Nb):
+    n = Ns * Nb
+    if prec in ("tf32x3", "bf16oz") and n not in (16, 32):
+        pytest.skip("tensor-core path covers n in {16, 32}")
+    cfg = Config(Ns=Ns, Nb=Nb, Nq=2, U=1.4, t2=0.3 if Nb > 1 else 0.0, EHM=True, vlaw="inv")
+    rng = np.random.default_rng(n + 7)
+    G1, XX, XY = physical_state(rng, Ns, Nb)
+    with g12.Context(params_of(g12, cfg), prec) as ctx:
+        got = ctx.rhs(G1, XX, XY, 1.3, 0.5, 2)
+    ref = oracle_rhs(oracle, cfg, G1, XX, XY, 1.3, 0.5, 2)
+    for k in ("h", "comm1", "Ix", "K1", "K2xx", "K2xy"):
+        assert rel_err(got[k], ref[k]) <= MIXED_RHS_TOL, (k, rel_err(got[k], ref[k]))
+
+
+def _run(g12, p, prec, G0, nsteps):
+    with g12.Context(p, prec) as ctx:
+        ctx.set_state(G0)
+        ctx.adiabatic_switch()
+        traj, rc = ctx.propagate(nsteps)
+        st = ctx.get_state()
+    return traj, rc, st
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16oz"])
+def test_mixed_propagation_vs_fp64_n16(g12, prec):
+    # configs[1] shape, adiabatic switching shortened so the run stays brief
+    cfg = Config(Ns=8, Nb=2, Nq=3, time_steps=300, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, vlaw="inv",
+                 q_type="pulse", quench_strength=2.0, quench_rate=2, quench_on_midpoint=15,
+                 quench_off_midpoint=25, AS_rate=0.3, AS_midpoint=2.0)
+    p = params_of(g12, cfg)
+    G0 = g12.make_G0(p)
+    ref, rc0, st0 = _run(g12, p, "fp64", G0, 300)
+    got, rc1, st1 = _run(g12, p, prec, G0, 300)
+    assert rc0 == 0 and rc1 == 0
+    assert rel_err(got, ref) <= TRAJ_TOL
+    # the G2 state itself agrees to single precision
+    assert rel_err(st1[1], st0[1]) <= 1e-4 and rel_err(st1[2], st0[2]) <= 1e-4
+
+
+def test_mixed_state_roundtrip_keeps_symmetry(g12):
+    rng = np.random.default_rng(5)
+    Ns, Nb = 8, 2
+    G1, XX, XY = physical_state(rng, Ns, Nb)
+    p = g12.make_params(Ns=Ns, Nb=Nb, U=1.0, t2=0.3)
+    with g12.Context(p, "bf16oz") as ctx:
+        ctx.set_state(G1, XX, XY)
+        g1, xx, xy = ctx.get_state()
+    assert np.array_equal(g1, G1.astype(complex))
+    assert rel_err(xx, XX) <= 1e-15 and rel_err(xy, XY) <= 1e-15
