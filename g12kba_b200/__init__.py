@@ -105,6 +105,18 @@ def lib():
         L.g12_kernel_name.argtypes = [C.c_void_p, C.c_int32]
         L.g12_fp64_peak_tflops.restype = C.c_double
         L.g12_fp64_peak_tflops.argtypes = [C.c_int32]
+        L.g12_batch_create.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+        L.g12_batch_destroy.argtypes = [C.c_void_p]
+        L.g12_batch_last_error.restype = C.c_char_p
+        L.g12_batch_last_error.argtypes = [C.c_void_p]
+        L.g12_batch_set_state.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
+        L.g12_batch_get_state.argtypes = [C.c_void_p, C.c_int32, _dp, _dp, _dp]
+        L.g12_batch_adiabatic_switch.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        L.g12_batch_propagate.argtypes = [C.c_void_p, C.c_int64, _dp, C.POINTER(C.c_int64)]
+        L.g12_batch_last_device_ms.restype = C.c_double
+        L.g12_batch_last_device_ms.argtypes = [C.c_void_p]
+        L.g12_batch_tile.restype = C.c_int32
+        L.g12_batch_tile.argtypes = [C.c_void_p, C.c_int32]
         L.g12_rhs_noalloc.argtypes = [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_double, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_char_p, C.c_int32]
@@ -280,6 +292,94 @@ class Context:
         calls = (C.c_int32 * 16)()
         nk = _check(lib().g12_kernel_times(self.h, nsteps, _ptr(avg), calls, 16), self.h)
         return {lib().g12_kernel_name(self.h, i).decode(): (float(avg[i]), int(calls[i])) for i in range(nk)}
+
+
+class Batch:
+    """An ensemble of independent systems advanced together (``g12_batch``)."""
+
+    def __init__(self, params, precision="fp64", device=0):
+        arr = (Params * len(params))(*params)
+        self.params = list(params)
+        self.nsys = len(params)
+        h = C.c_void_p()
+        rc = lib().g12_batch_create(arr, self.nsys, PREC[precision], device, C.byref(h))
+        if rc:
+            raise G12Error(f"g12_batch_create failed ({rc}): {lib().g12_batch_last_error(None).decode()}")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().g12_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc):
+        if rc < 0:
+            raise G12Error(f"libg12kba batch error {rc}: {lib().g12_batch_last_error(self.h).decode()}")
+        return rc
+
+    def set_state(self, i, G1, G2xx=None, G2xy=None):
+        n = self.params[i].n
+        G1 = _cx(G1, n * n)
+        G2xx = None if G2xx is None else _cx(G2xx, n ** 4)
+        G2xy = None if G2xy is None else _cx(G2xy, n ** 4)
+        self._chk(lib().g12_batch_set_state(self.h, i, _ptr(G1), _ptr(G2xx), _ptr(G2xy)))
+
+    def get_state(self, i):
+        n = self.params[i].n
+        G1 = np.zeros((n, n), np.complex128)
+        XX = np.zeros(n ** 4, np.complex128)
+        XY = np.zeros(n ** 4, np.complex128)
+        self._chk(lib().g12_batch_get_state(self.h, i, _ptr(G1), _ptr(XX), _ptr(XY)))
+        return G1, XX, XY
+
+    def adiabatic_switch(self):
+        done = C.c_int64()
+        self._chk(lib().g12_batch_adiabatic_switch(self.h, C.byref(done)))
+        return done.value
+
+    def propagate(self, nsteps):
+        """nsteps RK4 steps of every system; returns the dipoles (nsys, nsteps)."""
+        dip = np.zeros((self.nsys, max(nsteps, 1)))
+        done = C.c_int64()
+        self._chk(lib().g12_batch_propagate(self.h, nsteps, _ptr(dip), C.byref(done)))
+        return dip[:, :nsteps]
+
+    @property
+    def last_device_ms(self):
+        return float(lib().g12_batch_last_device_ms(self.h))
+
+    def tile(self, i):
+        return int(lib().g12_batch_tile(self.h, i))
+
+
+def ensemble_params(nsys=256, seed=20261203, time_steps=4000):
+    """The batched-ensemble configuration: Ns in {4,6,8,10,12}, Nb in {1,2},
+    U ~ U[0.5,2.5], t2 ~ U[0,0.5], quench strength ~ U[0.5,3] on Nq = Ns//3
+    sites; t1 = 1, EHM with w(r) = U/(1+r), dt = 0.01 (seeded MT19937)."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    out = []
+    for _ in range(nsys):
+        Ns = int(rng.choice([4, 6, 8, 10, 12]))
+        Nb = int(rng.choice([1, 2]))
+        U = float(rng.uniform(0.5, 2.5))
+        t2 = float(rng.uniform(0.0, 0.5))
+        qs = float(rng.uniform(0.5, 3.0))
+        out.append(make_params(Ns=Ns, Nb=Nb, Nq=Ns // 3, U=U, t1=1.0, t2=t2 if Nb > 1 else 0.0,
+                               quench_strength=qs, EHM=True, v_law="inv", dt=0.01, time_steps=time_steps,
+                               q_type="full"))
+    return out
 
 
 def fp64_peak_tflops(device=0) -> float:

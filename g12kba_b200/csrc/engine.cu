@@ -26,7 +26,7 @@ struct LaunchCfg {
     int ab_threads, cd_threads;
     size_t ab_smem, cd_smem, prep_smem, g1_smem;
     dim3 apply_grid;
-    int prep_blocks, g1_threads;
+    int prep_blocks, g1_blocks;
     int steps_per_graph;
 };
 
@@ -43,6 +43,8 @@ struct g12_ctx {
     LaunchCfg lc{};
     MixedState mixed{};
     cudaStream_t s = nullptr;
+    cudaStream_t s2 = nullptr;                 // side branch of the captured step (k_g1)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     StepP *sched_dev = nullptr;
@@ -201,13 +203,18 @@ int ensure_sched(g12_ctx *ctx, long long steps)
     return G12_OK;
 }
 
+// One RK4 step.  k_g1 of stage k only feeds k_prep of stage k+1, so it runs
+// on a side branch (s2) concurrently with the two-body kernels of stage k.
 void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
 {
     const LaunchCfg &lc = ctx->lc;
     k_step_begin<<<1, 256, 0, s>>>(d);
     for (int k = 0; k < 4; ++k) {
         k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, s>>>(d, k);
-        k_g1<<<1, lc.g1_threads, lc.g1_smem, s>>>(d, k);
+        cudaEventRecord(ctx->ev_fork, s);
+        cudaStreamWaitEvent(ctx->s2, ctx->ev_fork, 0);
+        k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s2>>>(d, k);
+        cudaEventRecord(ctx->ev_join, ctx->s2);
         if (d.gate) {
             if (ctx->prec == G12_PREC_FP64) {
                 k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, s>>>(d, k, lc.ab);
@@ -216,6 +223,7 @@ void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
                 mixed_enqueue_stage(ctx->mixed, d, k, ctx->prec, s);
             }
         }
+        cudaStreamWaitEvent(s, ctx->ev_join, 0);
     }
 }
 
@@ -338,7 +346,11 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
         ctx->err = "libg12kba is built for sm_100a (B200)";
         return fail(G12_ERR_NO_DEVICE);
     }
-    if (!ck(ctx, cudaStreamCreateWithFlags(&ctx->s, cudaStreamNonBlocking), "cudaStreamCreate")) return fail(G12_ERR_CUDA);
+    if (!ck(ctx, cudaStreamCreateWithFlags(&ctx->s, cudaStreamNonBlocking), "cudaStreamCreate") ||
+        !ck(ctx, cudaStreamCreateWithFlags(&ctx->s2, cudaStreamNonBlocking), "cudaStreamCreate") ||
+        !ck(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming), "cudaEventCreate") ||
+        !ck(ctx, cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming), "cudaEventCreate"))
+        return fail(G12_ERR_CUDA);
     cudaEventCreate(&ctx->ev0);
     cudaEventCreate(&ctx->ev1);
 
@@ -367,6 +379,7 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     // trajectory ring: up to 4096 snapshots or 1 GiB
     ctx->traj_cap = std::max<long long>(1, std::min<long long>(4096, (1LL << 30) / (n2 * 16)));
     d.traj_cap = ctx->traj_cap;
+    d.dip_cap = ctx->traj_cap;
     if (!dalloc(ctx, &d.traj, ctx->traj_cap * n2) || !dalloc(ctx, &d.dip, ctx->traj_cap)) return fail(G12_ERR_NOMEM);
 
     LaunchCfg &lc = ctx->lc;
@@ -377,10 +390,10 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     lc.ab_smem = (size_t(2) * lc.ab.NP * lc.ab.LD + size_t(lc.ab.NB) * lc.ab.NP * lc.ab.LD) * sizeof(double2);
     lc.cd_smem = lc.ab_smem + size_t(n) * n * sizeof(double2);
     lc.apply_grid = dim3(unsigned((n2 + lc.ab.NB - 1) / lc.ab.NB), 2, 1);
-    lc.prep_blocks = int((n2 + kPrepWarps - 1) / kPrepWarps);
-    lc.prep_smem = size_t(n2) * sizeof(double2) + size_t(kPrepWarps) * 4 * kMaxN * sizeof(double2);
-    lc.g1_threads = int(std::min<long long>(1024, (n2 + 31) / 32 * 32));
-    lc.g1_smem = size_t(2) * n2 * sizeof(double2);
+    lc.prep_blocks = prep_blocks(n2);
+    lc.prep_smem = prep_smem();
+    lc.g1_blocks = g1_blocks(n2);
+    lc.g1_smem = g1_smem(n2);
     lc.steps_per_graph = n <= 8 ? 8 : (n <= 16 ? 4 : 1);
     if (!ck(ctx, cudaFuncSetAttribute(k_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.ab_smem)), "attr") ||
         !ck(ctx, cudaFuncSetAttribute(k_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.cd_smem)), "attr") ||
@@ -390,6 +403,8 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     if (precision != G12_PREC_FP64) {
         int rc = mixed_init(ctx->mixed, d, precision, &ctx->err);
         if (rc) return fail(rc);
+        d.Qt = ctx->mixed.s.Qt;  // k_prep writes the transposed tables the epilogue reads
+        d.Rtt = ctx->mixed.s.Rtt;
     }
     if (ensure_sched(ctx, 1024)) return fail(G12_ERR_CUDA);
     *out = ctx;
@@ -408,6 +423,9 @@ extern "C" int g12_destroy(g12_ctx *ctx)
     if (ctx->sched_host) cudaFreeHost(ctx->sched_host);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->s2) cudaStreamDestroy(ctx->s2);
     if (ctx->s) cudaStreamDestroy(ctx->s);
     delete ctx;
     return G12_OK;
@@ -561,7 +579,7 @@ extern "C" int g12_rhs(g12_ctx *ctx, const double *G1, const double *G2xx, const
     CK(cudaMemsetAsync(dd.TMP0, 0, 2 * ctx->n4 * sizeof(double2), ctx->s));
     const LaunchCfg &lc = ctx->lc;
     k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, ctx->s>>>(dd, 0);
-    k_g1<<<1, lc.g1_threads, lc.g1_smem, ctx->s>>>(dd, 0);
+    k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s>>>(dd, 0);
     if (dd.gate) {
         if (ctx->prec == G12_PREC_FP64) {
             k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, ctx->s>>>(dd, 0, lc.ab);
@@ -645,7 +663,7 @@ extern "C" int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms
         timed(0, [&] { k_step_begin<<<1, 256, 0, ctx->s>>>(d); });
         for (int k = 0; k < 4; ++k) {
             timed(1, [&] { k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, ctx->s>>>(d, k); });
-            timed(2, [&] { k_g1<<<1, lc.g1_threads, lc.g1_smem, ctx->s>>>(d, k); });
+            timed(2, [&] { k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s>>>(d, k); });
             if (!d.gate) continue;
             if (ctx->prec == G12_PREC_FP64) {
                 timed(3, [&] { k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, ctx->s>>>(d, k, lc.ab); });

@@ -47,9 +47,11 @@ struct Dev {
     double law[kMaxN];  // V_m = U_eff * law[m-1], m = 1..nv
     double2 *Y1, *G1t0, *G1t1, *RK1, *h, *Ix, *comm_dbg, *K1_dbg;
     double2 *Y2, *RK2, *TMP0, *TMP1, *TAB, *D, *Q, *Rt;
+    double2 *Qt, *Rtt;  // transposed table copies (symmetric engine), or null
     double2 *traj;
     double *dip;
     long long traj_cap;
+    long long dip_cap;
     const StepP *sched;
     long long *counter, *limit;
     int *status, *active;
@@ -87,22 +89,17 @@ __device__ __forceinline__ double2 *g2_next(const Dev &d, int k) { return (k & 1
 // ---------------------------------------------------------------------------
 // Step head (RK_solver.h:98-110): copy this step's scalars, record the
 // snapshot and dipole, apply the site-0 density guard, stage-0 G1 input.
-__global__ void k_step_begin(Dev d)
+__device__ __forceinline__ void step_begin_body(const Dev &d)
 {
     __shared__ long long s_step;
     __shared__ int s_act, s_rec;
     const int tid = threadIdx.x;
     if (tid == 0) {
-        long long s = *d.counter;
-        int act = (*d.status == 0) && (s < *d.limit);
-        int rec = 0;
-        if (act) {
-            *d.cur = d.sched[s];
-            rec = d.sched[s].record;
-        }
+        const long long s = *d.counter;
+        const int act = (*d.status == 0) && (s < *d.limit);
         s_step = s;
         s_act = act;
-        s_rec = rec;
+        s_rec = act ? d.sched[s].record : 0;
     }
     __syncthreads();
     if (!s_act) {
@@ -111,9 +108,16 @@ __global__ void k_step_begin(Dev d)
     }
     const int n = d.n;
     const long long s = s_step;
+    {
+        // this step's scalars, one word per thread
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(d.sched + s);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(d.cur);
+        for (int w = tid; w < int(sizeof(StepP) / 4); w += blockDim.x) dst[w] = src[w];
+    }
     double2 *tr = d.traj + (s % d.traj_cap) * d.n2;
+#pragma unroll 4
     for (int x = tid; x < n * n; x += blockDim.x) {
-        double2 v = d.Y1[x];
+        const double2 v = d.Y1[x];
         d.G1t0[x] = v;
         if (s_rec) tr[x] = v;
     }
@@ -124,24 +128,27 @@ __global__ void k_step_begin(Dev d)
         for (int i = tid; i < n / 2; i += 32)
             acc += 2 * (sq / 2 - i - .5) * (d.Y1[i * (n + 1)].y - d.Y1[n * n - i * (n + 1) - 1].y) / sq;
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        if (tid == 0) d.dip[s % d.traj_cap] = acc;
-    }
-    if (tid == 0) {
-        int act = 1;
-        if (s_rec) {
-            double nd = 2 * d.Y1[0].y;
+        if (tid == 0) {
+            d.dip[s % d.dip_cap] = acc;
+            int act = 1;
+            const double nd = 2 * d.Y1[0].y;
             if (fabs(nd) > 3 || isnan(nd)) {
                 *d.status = int(s + 1);
                 act = 0;
             }
+            *d.active = act;
+            *d.counter = s + 1;
         }
-        *d.active = act;
+    } else if (tid == 0) {
+        *d.active = 1;
         *d.counter = s + 1;
     }
 }
 
+static __global__ void __launch_bounds__(256) k_step_begin(Dev d) { step_begin_body(d); }
+
 // HF.h:57-104, entry by entry.
-__device__ double2 h_entry(const Dev &d, const double2 *G, int mu, int nu, const StageP &st)
+__device__ __forceinline__ double2 h_entry(const Dev &d, const double2 *G, int mu, int nu, const StageP &st)
 {
     const int Ns = d.Ns, n = d.n;
     const int i = mu % Ns, a = mu / Ns, j = nu % Ns, b = nu / Ns;
@@ -179,148 +186,192 @@ __device__ double2 h_entry(const Dev &d, const double2 *G, int mu, int nu, const
 }
 
 // Per (alpha, beta) pair, one warp: Psi factor Rt, Pi factors Q_xx / Q_xy and
-// the collision integral.  Block 0 also builds h.
+// the collision integral; blocks past the pair blocks build h, one entry per
+// thread.  With d.Qt set (symmetric engine) the transposed copies
+// Qt[t][r][b][a] = Q[t][a][b][r] and Rtt[s][b][a] = Rt[a][b][s] are written too.
 constexpr int kPrepWarps = 4;
 
-__global__ void __launch_bounds__(kPrepWarps * 32) k_prep(Dev d, int k)
+__host__ __device__ inline int prep_pair_blocks(long long n2) { return int((n2 + kPrepWarps - 1) / kPrepWarps); }
+inline int prep_blocks(long long n2) { return prep_pair_blocks(n2) + int((n2 + kPrepWarps * 32 - 1) / (kPrepWarps * 32)); }
+inline size_t prep_smem() { return size_t(kPrepWarps) * 4 * kMaxN * sizeof(double2); }
+
+__device__ __forceinline__ void prep_body(const Dev &d, int k, int bx)
 {
     if (!*d.active) return;
     const StageP st = d.cur->st[k];
     const int n = d.n, Ns = d.Ns, Nb = d.Nb, nv = d.nv;
+    const long long n2 = (long long)n * n;
+    const double2 *__restrict__ G = g1_stage(d, k);
+    const int pair_blocks = prep_pair_blocks(n2);
+    if (bx >= pair_blocks) {
+        const long long x = (long long)(bx - pair_blocks) * blockDim.x + threadIdx.x;
+        if (x < n2) d.h[x] = h_entry(d, G, int(x / n), int(x % n), st);
+        return;
+    }
     extern __shared__ double2 sm[];
-    double2 *sG = sm;  // n*n
-    const double2 *G1 = g1_stage(d, k);
-    for (int x = threadIdx.x; x < n * n; x += blockDim.x) sG[x] = G1[x];
-    __syncthreads();
-    if (blockIdx.x == 0)
-        for (int x = threadIdx.x; x < n * n; x += blockDim.x) d.h[x] = h_entry(d, sG, x / n, x % n, st);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double2 *wE = sm + n * n + warp * (4 * kMaxN);   // n entries
-    double2 *wDx = wE + kMaxN;                         // n
-    double2 *wDy = wDx + kMaxN;                        // n
-    double2 *wS = wDy + kMaxN;                         // R / S, Ns entries
-    const long long pair = (long long)blockIdx.x * kPrepWarps + warp;
-    if (pair >= (long long)n * n) return;
+    double2 *wE = sm + warp * (4 * kMaxN);   // n entries
+    double2 *wDx = wE + kMaxN;               // n
+    double2 *wDy = wDx + kMaxN;              // n
+    double2 *wS = wDy + kMaxN;               // R / S, Ns entries
+    const long long pair = (long long)bx * kPrepWarps + warp;
+    if (pair >= n2) return;
     const int alpha = int(pair / n), beta = int(pair % n);
     const double U = st.U;
     if (!d.gate) {
         if (lane == 0) d.Ix[pair] = make_double2(0.0, 0.0);
         return;
     }
-    // R[s] = sum_r G1[alpha][(s,r)] G1[(s,r)][beta]
-    for (int r = lane; r < n; r += 32) wE[r] = c_mul(sG[alpha * n + r], sG[r * n + beta]);
-    __syncwarp();
-    double2 Rv[2];
-    for (int q = 0; q < 2; ++q) {
-        int s = lane + 32 * q;
-        double2 acc = make_double2(0.0, 0.0);
-        if (s < Ns)
-            for (int b = 0; b < Nb; ++b) acc = c_add(acc, wE[s + b * Ns]);
-        Rv[q] = acc;
-    }
-    __syncwarp();
-    for (int q = 0; q < 2; ++q) {
-        int s = lane + 32 * q;
-        if (s < Ns) wS[s] = Rv[q];
-    }
-    __syncwarp();
-    for (int s = lane; s < Ns; s += 32) {
-        double2 acc = c_scale(wS[s], U);
-        for (int m = 1; m <= nv; ++m) {
-            const double Vm = U * d.law[m - 1];
-            double2 t = make_double2(0.0, 0.0);
-            if (s + m < Ns) t = c_add(t, wS[s + m]);
-            if (s - m >= 0) t = c_add(t, wS[s - m]);
-            acc = c_add(acc, c_scale(t, Vm));
-        }
-        d.Rt[pair * Ns + s] = acc;
-    }
-    __syncwarp();
-    // D -> S -> Vp -> Q
+    // issue all global loads of this pair first: G rows/columns and the diagonals D
+    double2 ga[2], gb[2], dx[2], dy[2];
     const double2 *Dx = d.D + pair * n, *Dy = d.D + d.n3 + pair * n;
-    for (int r = lane; r < n; r += 32) {
-        wDx[r] = Dx[r];
-        wDy[r] = Dy[r];
-    }
-    __syncwarp();
-    double2 Sv[2];
+#pragma unroll
     for (int q = 0; q < 2; ++q) {
-        int s = lane + 32 * q;
-        double2 acc = make_double2(0.0, 0.0);
-        if (s < Ns)
-            for (int b = 0; b < Nb; ++b) acc = c_add(acc, c_add(wDx[s + b * Ns], wDy[s + b * Ns]));
-        Sv[q] = acc;
+        const int r = lane + 32 * q;
+        if (r < n) {
+            ga[q] = G[alpha * n + r];
+            gb[q] = G[r * n + beta];
+            dx[q] = Dx[r];
+            dy[q] = Dy[r];
+        }
     }
-    __syncwarp();
+#pragma unroll
     for (int q = 0; q < 2; ++q) {
-        int s = lane + 32 * q;
-        if (s < Ns) wS[s] = Sv[q];
+        const int r = lane + 32 * q;
+        if (r < n) {
+            wE[r] = c_mul(ga[q], gb[q]);  // G1[alpha][(s,b)] G1[(s,b)][beta]
+            wDx[r] = dx[q];
+            wDy[r] = dy[q];
+        }
     }
     __syncwarp();
-    double2 *wVp = wE;  // reuse: Ns entries
-    for (int s = lane; s < Ns; s += 32) {
-        double2 acc = make_double2(0.0, 0.0);
+    // R[s] = sum_b E[(s,b)],  S[s] = sum_b (Dxx + Dxy)[(s,b)]
+    double2 Rv[2], Sv[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int sidx = lane + 32 * q;
+        double2 r = make_double2(0.0, 0.0), sacc = make_double2(0.0, 0.0);
+        if (sidx < Ns)
+            for (int b = 0; b < Nb; ++b) {
+                r = c_add(r, wE[sidx + b * Ns]);
+                sacc = c_add(sacc, c_add(wDx[sidx + b * Ns], wDy[sidx + b * Ns]));
+            }
+        Rv[q] = r;
+        Sv[q] = sacc;
+    }
+    __syncwarp();
+    double2 *wR = wE;  // R over E (E no longer needed)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int sidx = lane + 32 * q;
+        if (sidx < Ns) {
+            wR[sidx] = Rv[q];
+            wS[sidx] = Sv[q];
+        }
+    }
+    __syncwarp();
+    // Rt[s] = U R[s] + sum_m V_m (R[s+m] + R[s-m]);  Vp[s] = sum_m V_m (S[s+m] + S[s-m])
+    double2 Vpv[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int sidx = lane + 32 * q;
+        Vpv[q] = make_double2(0.0, 0.0);
+        if (sidx >= Ns) continue;
+        double2 acc = c_scale(wR[sidx], U), vp = make_double2(0.0, 0.0);
         for (int m = 1; m <= nv; ++m) {
             const double Vm = U * d.law[m - 1];
-            double2 t = make_double2(0.0, 0.0);
-            if (s + m < Ns) t = c_add(t, wS[s + m]);
-            if (s - m >= 0) t = c_add(t, wS[s - m]);
-            acc = c_add(acc, c_scale(t, Vm));
+            double2 tr = make_double2(0.0, 0.0), ts = make_double2(0.0, 0.0);
+            if (sidx + m < Ns) {
+                tr = c_add(tr, wR[sidx + m]);
+                ts = c_add(ts, wS[sidx + m]);
+            }
+            if (sidx - m >= 0) {
+                tr = c_add(tr, wR[sidx - m]);
+                ts = c_add(ts, wS[sidx - m]);
+            }
+            acc = c_add(acc, c_scale(tr, Vm));
+            vp = c_add(vp, c_scale(ts, Vm));
         }
-        wVp[s] = acc;
+        d.Rt[pair * Ns + sidx] = acc;
+        if (d.Rtt) d.Rtt[((long long)sidx * n + beta) * n + alpha] = acc;
+        Vpv[q] = vp;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int sidx = lane + 32 * q;
+        if (sidx < Ns) wE[kMaxN - 1 - sidx] = Vpv[q];  // Vp stored from the top of wE (R no longer read)
     }
     __syncwarp();
     double2 *Qx = d.Q + pair * n, *Qy = d.Q + d.n3 + pair * n;
-    for (int r = lane; r < n; r += 32) {
-        const int s = r % Ns;
-        const double2 S = wS[s], vp = wVp[s];
-        double2 qx = c_mi(c_add(c_scale(c_sub(S, wDx[r]), U), vp));
-        double2 qy = c_mi(c_add(c_scale(c_sub(S, wDy[r]), U), vp));
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int r = lane + 32 * q;
+        if (r >= n) continue;
+        const int sidx = r % Ns;
+        const double2 S = wS[sidx], vp = wE[kMaxN - 1 - sidx];
+        const double2 qx = c_mi(c_add(c_scale(c_sub(S, wDx[r]), U), vp));
+        const double2 qy = c_mi(c_add(c_scale(c_sub(S, wDy[r]), U), vp));
         Qx[r] = qx;
         Qy[r] = qy;
+        if (d.Qt) {
+            d.Qt[((long long)r * n + beta) * n + alpha] = qx;
+            d.Qt[d.n3 + ((long long)r * n + beta) * n + alpha] = qy;
+        }
         if (r == alpha) d.Ix[pair] = qx;
     }
 }
 
+static __global__ void __launch_bounds__(kPrepWarps * 32) k_prep(Dev d, int k) { prep_body(d, k, blockIdx.x); }
+
 // G1 side of a stage (commutators.h:28-51, G1_G2_t_step.h:24-47) and the
-// G1 RK bookkeeping (RK_solver.h:134-135, 204-208).  One block.
-__global__ void __launch_bounds__(1024) k_g1(Dev d, int k)
+// G1 RK bookkeeping (RK_solver.h:134-135, 204-208).  One output per thread,
+// blocks of 128; each block stages h and G1 in shared memory.
+constexpr int kG1Threads = 128;
+inline int g1_blocks(long long n2) { return int((n2 + kG1Threads - 1) / kG1Threads); }
+inline size_t g1_smem(long long n2) { return size_t(2) * n2 * sizeof(double2); }
+
+__device__ __forceinline__ void g1_body(const Dev &d, int k, int bx)
 {
     if (!*d.active) return;
     const StageP st = d.cur->st[k];
     const int n = d.n;
+    const int n2 = n * n;
     extern __shared__ double2 sm[];
-    double2 *sH = sm, *sG = sm + n * n;
+    double2 *sH = sm, *sG = sm + n2;
     const double2 *G1 = g1_stage(d, k);
-    for (int x = threadIdx.x; x < n * n; x += blockDim.x) {
+#pragma unroll 4
+    for (int x = threadIdx.x; x < n2; x += blockDim.x) {
         sH[x] = d.h[x];
         sG[x] = G1[x];
     }
     __syncthreads();
+    const int x = bx * blockDim.x + threadIdx.x;
+    if (x >= n2) return;
     double2 *G1n = g1_next(d, k);
-    for (int x = threadIdx.x; x < n * n; x += blockDim.x) {
-        const int mu = x / n, nu = x % n;
-        double2 hg = make_double2(0.0, 0.0), gh = make_double2(0.0, 0.0);
-        for (int r = 0; r < n; ++r) {
-            hg = c_mac(hg, sH[mu * n + r], sG[r * n + nu]);
-            gh = c_mac(gh, sG[mu * n + r], sH[r * n + nu]);
-        }
-        const double2 comm = c_sub(hg, gh);
-        const double2 K = c_mi(c_add(c_add(comm, d.Ix[x]), c_conj(d.Ix[nu * n + mu])));
-        if (d.debug) {
-            d.comm_dbg[x] = comm;
-            d.K1_dbg[x] = K;
-            continue;
-        }
-        const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : d.RK1[x], c_scale(K, st.w));
-        if (k < 3) {
-            d.RK1[x] = rk;
-            G1n[x] = c_add(d.Y1[x], c_scale(K, st.c_next));
-        } else {
-            d.Y1[x] = c_add(d.Y1[x], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
-        }
+    const int mu = x / n, nu = x % n;
+    double2 hg = make_double2(0.0, 0.0), gh = make_double2(0.0, 0.0);
+    for (int r = 0; r < n; ++r) {
+        hg = c_mac(hg, sH[mu * n + r], sG[r * n + nu]);
+        gh = c_mac(gh, sG[mu * n + r], sH[r * n + nu]);
+    }
+    const double2 comm = c_sub(hg, gh);
+    const double2 K = c_mi(c_add(c_add(comm, d.Ix[x]), c_conj(d.Ix[nu * n + mu])));
+    if (d.debug) {
+        d.comm_dbg[x] = comm;
+        d.K1_dbg[x] = K;
+        return;
+    }
+    const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : d.RK1[x], c_scale(K, st.w));
+    if (k < 3) {
+        d.RK1[x] = rk;
+        G1n[x] = c_add(d.Y1[x], c_scale(K, st.c_next));
+    } else {
+        d.Y1[x] = c_add(d.Y1[x], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
     }
 }
+
+static __global__ void __launch_bounds__(kG1Threads) k_g1(Dev d, int k) { g1_body(d, k, blockIdx.x); }
 
 // Two-body commutator halves as Y = L X + X R on a batch of n x n matrices
 // held in shared memory ("natural" layout: row = slower index).
@@ -337,13 +388,12 @@ struct ApplyCfg {
 };
 
 template <bool CD>
-__global__ void __launch_bounds__(256) k_apply(Dev d, int k, ApplyCfg cfg)
+__device__ __forceinline__ void apply_body(const Dev &d, int k, const ApplyCfg &cfg, int bx, int t)
 {
     if (!*d.active) return;
     const int n = d.n, NP = cfg.NP, LD = cfg.LD, S = cfg.S, NB = cfg.NB;
     const long long n2 = d.n2, n4 = d.n4;
-    const int t = blockIdx.y;
-    const long long m0 = (long long)blockIdx.x * NB;
+    const long long m0 = (long long)bx * NB;
     const int nm = int(min((long long)NB, n2 - m0));
     extern __shared__ double2 sm[];
     double2 *Hs = sm, *HTs = sm + NP * LD, *Xs = sm + 2 * NP * LD;
@@ -503,8 +553,14 @@ __global__ void __launch_bounds__(256) k_apply(Dev d, int k, ApplyCfg cfg)
     }
 }
 
+template <bool CD>
+static __global__ void __launch_bounds__(256) k_apply(Dev d, int k, ApplyCfg cfg)
+{
+    apply_body<CD>(d, k, cfg, blockIdx.x, blockIdx.y);
+}
+
 // D[t][a][b][r] = Y2_t[a, r; b, r]
-__global__ void k_init_D(Dev d)
+static __global__ void k_init_D(Dev d)
 {
     const long long total = 2 * d.n3;
     const int n = d.n;
@@ -528,14 +584,14 @@ __device__ __forceinline__ long long ref_index(int Ns, int Nb, long long x, int 
            (a + (long long)b * Nb) * Ns2 * Ns2 * Nb2;
 }
 
-__global__ void k_from_ref(const double2 *__restrict__ src, double2 *__restrict__ dst, int Ns, int Nb, long long n4)
+static __global__ void k_from_ref(const double2 *__restrict__ src, double2 *__restrict__ dst, int Ns, int Nb, long long n4)
 {
     const int n = Ns * Nb;
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n4; x += (long long)gridDim.x * blockDim.x)
         dst[x] = src[ref_index(Ns, Nb, x, n)];
 }
 
-__global__ void k_to_ref(const double2 *__restrict__ src, double2 *__restrict__ dst, int Ns, int Nb, long long n4)
+static __global__ void k_to_ref(const double2 *__restrict__ src, double2 *__restrict__ dst, int Ns, int Nb, long long n4)
 {
     const int n = Ns * Nb;
     for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n4; x += (long long)gridDim.x * blockDim.x)

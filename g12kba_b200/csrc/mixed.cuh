@@ -27,7 +27,7 @@ struct MixedState {
     SymDev s{};
     CUtensorMap map_a{}, map_b{};  // TMA views of TMPa / TMPb
     size_t epi_smem = 0, simt_smem = 0, tc_smem = 0;
-    int tc_grid = 0, tables_grid = 0;
+    int tc_grid = 0;
     std::vector<void *> allocs;
 };
 
@@ -141,10 +141,12 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
     s.gemm_c = gc;
     s.gemm_partner = gp;
     s.pairs = pp;
-    m.epi_smem = size_t(n2) * sizeof(double2) + 2 * kTB * (kTB + 1) * sizeof(float2) + kTB * kTB * sizeof(double2);
+    m.epi_smem = size_t(n) * (n + 1) * sizeof(double2) + 2 * kTB * (kTB + 1) * sizeof(float2) + kTB * (kTB + 1) * sizeof(double2);
     m.simt_smem = (size_t(128) * 2 * n + size_t(128) * (2 * n + 1)) * sizeof(float) + size_t(n2) * sizeof(float2);
-    m.tables_grid = int(std::min<long long>(4096, (2 * n3 + n2 * d.Ns + 255) / 256));
-    cudaFuncSetAttribute(k_sym_epi, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+    cudaFuncSetAttribute(k_sym_epi<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+    cudaFuncSetAttribute(k_sym_epi<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+    cudaFuncSetAttribute(k_sym_epi<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+    cudaFuncSetAttribute(k_sym_epi<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
     cudaFuncSetAttribute(k_sym_gemm_simt, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.simt_smem));
     if (m.tc) {
         if (!encode_tmp_map(&m.map_a, s.TMPa, n, err) || !encode_tmp_map(&m.map_b, s.TMPb, n, err)) return -2;
@@ -202,13 +204,12 @@ inline int mixed_to_full(MixedState &m, const Dev &d, cudaStream_t st)
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
-inline int mixed_kernel_kinds(const MixedState &) { return 3; }
+inline int mixed_kernel_kinds(const MixedState &) { return 2; }
 
 inline const char *mixed_kernel_name(const MixedState &m, int q)
 {
-    if (q == 0) return "k_sym_tables";
-    if (q == 1) return m.oz ? "k_sym_gemm_oz" : (m.tc ? "k_sym_gemm_tc" : "k_sym_gemm_simt");
-    if (q == 2) return "k_sym_epi";
+    if (q == 0) return m.oz ? "k_sym_gemm_oz" : (m.tc ? "k_sym_gemm_tc" : "k_sym_gemm_simt");
+    if (q == 1) return "k_sym_epi";
     return "";
 }
 
@@ -217,12 +218,10 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
     m.s.d = d;
     const SymDev &s = m.s;
     if (q == 0) {
-        k_sym_tables<<<m.tables_grid, 256, 0, st>>>(s);
-    } else if (q == 1) {
         if (m.tc) {
             const CUtensorMap &map = (k & 1) ? m.map_a : m.map_b;
-            if (m.oz && s.n == 32) k_sym_gemm_oz<32><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k);
-            else if (m.oz) k_sym_gemm_oz<16><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k);
+            if (m.oz && s.n == 32) k_sym_gemm_oz<32><<<m.tc_grid, kOzThreads, m.tc_smem, st>>>(s, k);
+            else if (m.oz) k_sym_gemm_oz<16><<<m.tc_grid, kOzThreads, m.tc_smem, st>>>(s, k);
             else if (s.n == 32 && m.pieces == 2) k_sym_gemm_tc<32, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (s.n == 32) k_sym_gemm_tc<32, 3><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (m.pieces == 2) k_sym_gemm_tc<16, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
@@ -231,16 +230,20 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
             k_sym_gemm_simt<<<2 * s.gemm_tiles, 256, m.simt_smem, st>>>(s, k);
         }
     } else {
-        k_sym_epi<<<dim3(s.npairs, 2), 256, m.epi_smem, st>>>(s, k);
+        const dim3 g(s.npairs, 2);
+        if (s.n == 32) k_sym_epi<32><<<g, 256, m.epi_smem, st>>>(s, k);
+        else if (s.n == 16) k_sym_epi<16><<<g, 256, m.epi_smem, st>>>(s, k);
+        else if (s.n == 8) k_sym_epi<8><<<g, 256, m.epi_smem, st>>>(s, k);
+        else k_sym_epi<64><<<g, 256, m.epi_smem, st>>>(s, k);
     }
 }
 
 inline void mixed_enqueue_stage(MixedState &m, const Dev &d, int k, int prec, cudaStream_t st)
 {
-    for (int q = 0; q < 3; ++q) mixed_enqueue_kind(m, d, k, prec, q, st);
+    for (int q = 0; q < 2; ++q) mixed_enqueue_kind(m, d, k, prec, q, st);
 }
 
-inline int mixed_launches_per_stage(const MixedState &) { return 3; }
+inline int mixed_launches_per_stage(const MixedState &) { return 2; }
 
 // device error word of the bounded waits (0: none)
 inline int mixed_error(MixedState &m)

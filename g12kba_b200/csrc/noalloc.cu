@@ -112,11 +112,11 @@ int setup_device(int dev, void **base, std::string *msg)
             return G12_ERR_CUDA;
         }
         const Cfg c = apply_cfg(kMax);
-        const size_t prep = kN2 * sizeof(double2) + size_t(K::kPrepWarps) * 4 * K::kMaxN * sizeof(double2);
+        const size_t prep = K::prep_smem();
         if ((e = cudaFuncSetAttribute(K::k_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c.ab_smem))) ||
             (e = cudaFuncSetAttribute(K::k_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(c.cd_smem))) ||
             (e = cudaFuncSetAttribute(K::k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(prep))) ||
-            (e = cudaFuncSetAttribute(K::k_g1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(2 * kN2 * sizeof(double2))))) {
+            (e = cudaFuncSetAttribute(K::k_g1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(K::g1_smem(kN2))))) {
             *msg = std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e);
             return G12_ERR_CUDA;
         }
@@ -214,9 +214,8 @@ extern "C" int g12_rhs_noalloc(const g12_params *p, const double *G1_dev, const 
         sp.st[k].w = 1;
     }
     const Cfg c = apply_cfg(n);
-    const int prep_blocks = int((n2 + K::kPrepWarps - 1) / K::kPrepWarps);
-    const size_t prep_smem = size_t(n2) * sizeof(double2) + size_t(K::kPrepWarps) * 4 * K::kMaxN * sizeof(double2);
-    const int g1_threads = int(std::min<long long>(1024, (n2 + 31) / 32 * 32));
+    const int prep_blocks = K::prep_blocks(n2);
+    const size_t prep_smem = K::prep_smem();
     const dim3 grid(unsigned((n2 + c.a.NB - 1) / c.a.NB), 2, 1);
 
     k_noalloc_params<<<1, 1, 0, s>>>(sp, d.cur, d.active);
@@ -224,7 +223,7 @@ extern "C" int g12_rhs_noalloc(const g12_params *p, const double *G1_dev, const 
     K::k_from_ref<<<64, 256, 0, s>>>(reinterpret_cast<const double2 *>(G2xy_dev), d.Y2 + n4, Ns, Nb, n4);
     K::k_init_D<<<64, 256, 0, s>>>(d);
     K::k_prep<<<prep_blocks, K::kPrepWarps * 32, prep_smem, s>>>(d, 0);
-    K::k_g1<<<1, g1_threads, 2 * n2 * sizeof(double2), s>>>(d, 0);
+    K::k_g1<<<K::g1_blocks(n2), K::kG1Threads, K::g1_smem(n2), s>>>(d, 0);
     if (d.gate) {
         K::k_apply<false><<<grid, c.threads, c.ab_smem, s>>>(d, 0, c.a);
         K::k_apply<true><<<grid, c.threads, c.cd_smem, s>>>(d, 0, c.a);

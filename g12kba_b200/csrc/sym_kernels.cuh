@@ -55,28 +55,6 @@ __device__ __forceinline__ long long tmp_index(int n, int mu1, int mu2, int c, i
     return (((long long)mu2 * n * n + c) * 2 + part) * n + mu1;
 }
 
-// Transposed table copies for coalesced epilogue reads: Qt[t][r][b][a] = Q[t][a][b][r],
-// Rtt[s][b][a] = Rt[a][b][s].  One thread per element.
-__global__ void k_sym_tables(SymDev s)
-{
-    if (!*s.d.active || !s.d.gate) return;
-    const int n = s.n, Ns = s.d.Ns;
-    const long long n3 = (long long)n * n * n;
-    const long long tot = 2 * n3 + (long long)n * n * Ns;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
-        if (e < 2 * n3) {
-            const int t = int(e / n3);
-            const long long q = e % n3;  // output index: (r*n + b)*n + a
-            const int a = int(q % n), b = int((q / n) % n), r = int(q / ((long long)n * n));
-            s.Qt[t * n3 + q] = s.d.Q[t * n3 + ((long long)a * n + b) * n + r];
-        } else {
-            const long long q = e - 2 * n3;  // (s*n + b)*n + a
-            const int a = int(q % n), b = int((q / n) % n), sidx = int(q / ((long long)n * n));
-            s.Rtt[q] = s.d.Rt[((long long)a * n + b) * Ns + sidx];
-        }
-    }
-}
-
 // Reference FP32 SIMT version of the W contraction (same tiles as the
 // tensor-core kernel): T1[mu1][mu2][c] = sum_rho h[mu1][rho] X[rho][mu2][c].
 __global__ void __launch_bounds__(256) k_sym_gemm_simt(SymDev s, int k)
@@ -131,11 +109,15 @@ __global__ void __launch_bounds__(256) k_sym_gemm_simt(SymDev s, int k)
 // Stage epilogue on a tile pair (R, C) / (C, R): C = W - W^H, Psi, Pi, K2,
 // RK4 bookkeeping on the compressed state, next-stage input (both tiles, FP32),
 // particle-2 diagonal D (FP64).
+template <int NN>
 __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
 {
     if (!*s.d.active) return;
     const Dev &d = s.d;
-    const int n = s.n, Ns = d.Ns;
+    constexpr int n = NN;
+    constexpr int GLD = NN + 1;   // padded G1 rows (bank-conflict-free column reads)
+    constexpr int KLD = kTB + 1;  // padded K rows
+    const int Ns = d.Ns;
     const long long n2 = (long long)n * n, n3 = n2 * n;
     const int t = blockIdx.y;
     const int p = blockIdx.x;
@@ -143,13 +125,17 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
     const int R0 = rc.x * kTB, C0 = rc.y * kTB;
     const bool diag = rc.x == rc.y;
     extern __shared__ double2 smd[];
-    double2 *Gs = smd;                                 // n*n
-    float2 *Wrc = reinterpret_cast<float2 *>(Gs + n * n);  // [c_l][r_l] = W[R0+r_l][C0+c_l]
+    double2 *Gs = smd;                                 // n x GLD
+    float2 *Wrc = reinterpret_cast<float2 *>(Gs + n * GLD);  // [c_l][r_l] = W[R0+r_l][C0+c_l]
     float2 *Wcr = Wrc + kTB * (kTB + 1);               // [r_l][c_l] = W[C0+c_l][R0+r_l]
-    double2 *Ks = reinterpret_cast<double2 *>(Wcr + kTB * (kTB + 1));  // [c_l][r_l] tmp_next (or K)
+    double2 *Ks = reinterpret_cast<double2 *>(Wcr + kTB * (kTB + 1));  // [c_l][r_l] tmp_next (or K), rows of KLD
+    __shared__ int site[NN];
     const float *Wg = s.W + t * 2 * s.n4;
     const double2 *G1 = (k & 1) ? d.G1t1 : d.G1t0;
-    for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[x] = G1[x];
+    if (threadIdx.x < NN) site[threadIdx.x] = threadIdx.x % Ns;
+#pragma unroll 4
+    for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[(x / n) * GLD + x % n] = G1[x];
+#pragma unroll
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
         // W[R0+rl][C0+cl] at (c*2+part)*n2 + r: contiguous in rl
@@ -163,13 +149,16 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
 
     const StageP st = d.cur->st[k];
     const double U = st.U;
-    const double2 *Qo = d.Q + t * n3, *Qt = s.Qt + t * n3;
+    const double2 *__restrict__ Qo = d.Q + t * n3;
+    const double2 *__restrict__ Qt = s.Qt + t * n3;
+    const double2 *__restrict__ Rtt = s.Rtt;
     double2 *Yc = s.Yc + ((long long)t * s.npairs + p) * kTB * kTB;
     double2 *Ac = s.Ac + ((long long)t * s.npairs + p) * kTB * kTB;
     auto vdist = [&](int s1, int s2) -> double {
         const int m = abs(s1 - s2);
         return (m >= 1 && m <= d.nv) ? U * d.law[m - 1] : 0.0;
     };
+#pragma unroll 4
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
         const int r = R0 + rl, c = C0 + cl;
@@ -178,26 +167,25 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
         // W[c][r] = Wcr at (row offset cl in block C -> index rl' = cl, col r -> cl' = rl)
         const float2 w2 = Wcr[rl * (kTB + 1) + cl];
         const double2 C = make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
-        const int si = mu1 % Ns, sj = mu2 % Ns, sk = nu1 % Ns, sl = nu2 % Ns;
-        const double2 g11 = Gs[mu1 * n + nu1], g22 = Gs[mu2 * n + nu2];
+        const int si = site[mu1], sj = site[mu2], sk = site[nu1], sl = site[nu2];
+        const double2 g11 = Gs[mu1 * GLD + nu1], g22 = Gs[mu2 * GLD + nu2];
         const double wd = (U * double(si == sj) + vdist(si, sj)) - (U * double(sk == sl) + vdist(sk, sl));
         double2 psi = c_scale(c_mul(g11, g22), wd);
-        const double2 *Rtt = s.Rtt;
         psi = c_add(psi, c_i(c_mul(g22, c_sub(Rtt[((long long)sj * n + nu1) * n + mu1], Rtt[((long long)sl * n + nu1) * n + mu1]))));
         const double2 *Rt2 = d.Rt + ((long long)mu2 * n + nu2) * Ns;
         psi = c_add(psi, c_i(c_mul(g11, c_sub(Rt2[si], Rt2[sk]))));
         if (t == 0) {
             psi = c_sub(psi, c_scale(c_mul(g11, g22), U * (double(mu1 == mu2) - double(nu1 == nu2))));
-            const double2 e1 = c_sub(c_mul(Gs[mu1 * n + mu2], Gs[mu2 * n + nu1]), c_mul(Gs[mu1 * n + nu2], Gs[nu2 * n + nu1]));
-            const double2 e2 = c_sub(c_mul(Gs[mu2 * n + mu1], Gs[mu1 * n + nu2]), c_mul(Gs[mu2 * n + nu1], Gs[nu1 * n + nu2]));
+            const double2 e1 = c_sub(c_mul(Gs[mu1 * GLD + mu2], Gs[mu2 * GLD + nu1]), c_mul(Gs[mu1 * GLD + nu2], Gs[nu2 * GLD + nu1]));
+            const double2 e2 = c_sub(c_mul(Gs[mu2 * GLD + mu1], Gs[mu1 * GLD + nu2]), c_mul(Gs[mu2 * GLD + nu1], Gs[nu1 * GLD + nu2]));
             psi = c_add(psi, c_scale(c_mi(c_add(c_mul(g22, e1), c_mul(g11, e2))), U));
         }
         // Pi[x] = G1[mu2][nu2] (Q[mu1][nu1][mu2] - Q[mu1][nu1][nu2]); Qt[r][b][a] = Q[a][b][r]
         const double2 pi = c_mul(g22, c_sub(Qt[((long long)mu2 * n + nu1) * n + mu1], Qt[((long long)nu2 * n + nu1) * n + mu1]));
         const long long q2 = ((long long)nu2 * n + mu2) * n;
-        const double2 piP = c_mul(Gs[nu1 * n + mu1], c_sub(Qo[q2 + nu1], Qo[q2 + mu1]));
+        const double2 piP = c_mul(Gs[nu1 * GLD + mu1], c_sub(Qo[q2 + nu1], Qo[q2 + mu1]));
         const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
-        Ks[cl * kTB + rl] = K;
+        Ks[cl * KLD + rl] = K;
     }
     __syncthreads();
     if (diag) {
@@ -206,14 +194,14 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
         int cnt = 0;
         for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
             const int rl = e % kTB, cl = e / kTB;
-            const double2 a = Ks[cl * kTB + rl], b = c_conj(Ks[rl * kTB + cl]);
+            const double2 a = Ks[cl * KLD + rl], b = c_conj(Ks[rl * KLD + cl]);
             sym[cnt++] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
         }
         __syncthreads();
         cnt = 0;
         for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
             const int rl = e % kTB, cl = e / kTB;
-            Ks[cl * kTB + rl] = sym[cnt++];
+            Ks[cl * KLD + rl] = sym[cnt++];
         }
         __syncthreads();
     }
@@ -222,7 +210,7 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
         double2 *Kd = d.Y2 + t * n2 * n2;
         for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
             const int rl = e % kTB, cl = e / kTB;
-            const double2 K = Ks[cl * kTB + rl];
+            const double2 K = Ks[cl * KLD + rl];
             Kd[(long long)(R0 + rl) * n2 + C0 + cl] = K;
             Kd[(long long)(C0 + cl) * n2 + R0 + rl] = c_conj(K);
         }
@@ -232,7 +220,7 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
     double2 *Dt = d.D + t * n3;
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
-        const double2 K = Ks[cl * kTB + rl];
+        const double2 K = Ks[cl * KLD + rl];
         const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : Ac[e], c_scale(K, st.w));
         double2 v;
         if (k < 3) {
@@ -242,7 +230,7 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
             v = c_add(Yc[e], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
             Yc[e] = v;
         }
-        Ks[cl * kTB + rl] = v;
+        Ks[cl * KLD + rl] = v;
         const int r = R0 + rl, c = C0 + cl;
         const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
         if (mu2 == nu2) {
@@ -257,7 +245,7 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
         const int r = R0 + rl, c = C0 + cl;
-        const double2 v = Ks[cl * kTB + rl];
+        const double2 v = Ks[cl * KLD + rl];
         const long long o = tmp_index(n, r % n, r / n, c, 0);
         Out[o] = float(v.x);
         Out[o + n] = float(v.y);
@@ -267,7 +255,7 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
         for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
             const int cl = e % kTB, rl = e / kTB;
             const int r = R0 + rl, c = C0 + cl;
-            const double2 v = Ks[cl * kTB + rl];
+            const double2 v = Ks[cl * KLD + rl];
             const long long o = tmp_index(n, c % n, c / n, r, 0);
             Out[o] = float(v.x);
             Out[o + n] = float(-v.y);

@@ -64,6 +64,31 @@ __device__ __forceinline__ void oz_digits(float x, float (&d)[kOzDigits])
     d[3] = rintf(r * 128.0f);
 }
 
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }  // |e| < 127
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <int W>
+__device__ __forceinline__ void tmem_ldw(uint32_t taddr, float (&v)[W])
+{
+    if constexpr (W == 32) tmem_ld32(taddr, v);
+    else tmem_ld16(taddr, v);
+}
+
+constexpr int kOzThreads = 256;
+
 template <int NN>
 struct OzShape {
     static constexpr int N = 2 * NN;           // UMMA N
@@ -77,12 +102,15 @@ struct OzShape {
     static constexpr int OFF_A = 0;                               // kOzDigits x A_BYTES
     static constexpr int OFF_B = kOzDigits * A_BYTES;             // kOzDigits x B_BYTES
     static constexpr int OFF_EA = OFF_B + kOzDigits * B_BYTES;    // 128 ints
-    static constexpr int OFF_EB = OFF_EA + 128 * 4;               // N ints
-    static constexpr int OFF_BAR = OFF_EB + 256 * 4;
+    static constexpr int OFF_EB = OFF_EA + 128 * 4;               // N ints, then N doubles (scales)
+    static constexpr int OFF_BAR = OFF_EB + 256 * 4 + 128 * 8;
     static constexpr int SMEM = OFF_BAR + 64 + 1024;
     static constexpr int S_LD = N + 1;
     static constexpr int LPR = K * 4 / 16;    // lanes per FP32 row (16-byte loads): 16 or 8
     static constexpr int RPW = 32 / LPR;      // rows per warp load: 2 or 4
+    static constexpr int WARPS = kOzThreads / 32;
+    static constexpr int ITER = 128 / (WARPS * RPW);  // row loads per warp per tile
+    static constexpr int HALF = N / 2;                // TMEM columns per warp (two warps per lane quadrant)
     static_assert(128 * S_LD * 4 <= kOzDigits * A_BYTES, "staging must fit in the digit buffers");
     static_assert(TMEM_COLS <= 256, "two CTAs per SM share 512 TMEM columns");
 };
@@ -93,7 +121,7 @@ __device__ __forceinline__ int swz_byte(int row, int kk2)  // bf16 element kk2 o
 }
 
 template <int NN>
-__global__ void __launch_bounds__(128) k_sym_gemm_oz(SymDev s, int k)
+__global__ void __launch_bounds__(kOzThreads, 2) k_sym_gemm_oz(SymDev s, int k)
 {
     using Sh = OzShape<NN>;
     if (!*s.d.active) return;
@@ -122,37 +150,45 @@ __global__ void __launch_bounds__(128) k_sym_gemm_oz(SymDev s, int k)
     // zero the digit buffers once (the n = 16 rows use half of each 128-byte row)
     for (int i = tid; i < (Sh::OFF_EA) / 16; i += blockDim.x) reinterpret_cast<uint4 *>(sm)[i] = make_uint4(0, 0, 0, 0);
     __syncthreads();
-    // B digits: rows j of the real form of h^T (FP64), one thread per row
+    // B digits: rows j of the real form of h^T (FP64).  h is staged in the (not
+    // yet used) A digit area, then one thread per row finds the row maximum and
+    // all threads write digits.
+    double2 *hs = reinterpret_cast<double2 *>(Ad);
+#pragma unroll 4
+    for (int x = tid; x < NN * NN; x += blockDim.x) hs[x] = s.d.h[x];
+    __syncthreads();
+    auto bval = [&](int j, int kk) -> double {
+        const int po = j / NN, mu1 = j % NN, pi = kk / NN, rho = kk % NN;
+        const double2 hv = hs[mu1 * NN + rho];
+        return (po == 0) ? ((pi == 0) ? hv.x : -hv.y) : ((pi == 0) ? hv.y : hv.x);
+    };
+    double *sB = reinterpret_cast<double *>(sm + Sh::OFF_EB + 256 * 4);  // per-row scale 2^(e_j - 6)
     for (int j = tid; j < Sh::N; j += blockDim.x) {
-        const int po = j / NN, mu1 = j % NN;
         double mx = 0.0;
-        for (int kk = 0; kk < Sh::K; ++kk) {
-            const int pi = kk / NN, rho = kk % NN;
-            const double2 hv = s.d.h[mu1 * NN + rho];
-            const double v = (po == 0) ? ((pi == 0) ? hv.x : -hv.y) : ((pi == 0) ? hv.y : hv.x);
-            mx = fmax(mx, fabs(v));
-        }
+        for (int kk = 0; kk < Sh::K; ++kk) mx = fmax(mx, fabs(bval(j, kk)));
         const int e = (mx > 0.0) ? ilogb(mx) : 0;
         eB[j] = e;
-        for (int kk = 0; kk < Sh::K; ++kk) {
-            const int pi = kk / NN, rho = kk % NN;
-            const double2 hv = s.d.h[mu1 * NN + rho];
-            const double v = (po == 0) ? ((pi == 0) ? hv.x : -hv.y) : ((pi == 0) ? hv.y : hv.x);
-            // |v * 2^(20-e)| < 2^21; the first digit and remainders are exact in FP64 before rounding to FP32
-            double r = ldexp(v, 20 - e);
-            float d[kOzDigits];
-            d[0] = float(rint(r / 16384.0));
-            r -= double(d[0]) * 16384.0;
-            d[1] = float(rint(r / 128.0));
-            r -= double(d[1]) * 128.0;
-            d[2] = float(rint(r));
-            r -= double(d[2]);
-            d[3] = float(rint(r * 128.0));
-#pragma unroll
-            for (int q = 0; q < kOzDigits; ++q)
-                *reinterpret_cast<__nv_bfloat16 *>(Bd + q * Sh::B_BYTES + swz_byte(j, kk)) = __float2bfloat16_rn(d[q]);
-        }
+        sB[j] = ldexp(1.0, e - 6);
     }
+    __syncthreads();
+    for (int x = tid; x < Sh::N * Sh::K; x += blockDim.x) {
+        const int jj = x / Sh::K, kk = x % Sh::K;
+        double r = ldexp(bval(jj, kk), 20 - eB[jj]);
+        float d[kOzDigits];
+        d[0] = float(rint(r / 16384.0));
+        r -= double(d[0]) * 16384.0;
+        d[1] = float(rint(r / 128.0));
+        r -= double(d[1]) * 128.0;
+        d[2] = float(rint(r));
+        r -= double(d[2]);
+        d[3] = float(rint(r * 128.0));
+#pragma unroll
+        for (int q = 0; q < kOzDigits; ++q)
+            *reinterpret_cast<__nv_bfloat16 *>(Bd + q * Sh::B_BYTES + swz_byte(jj, kk)) = __float2bfloat16_rn(d[q]);
+    }
+    __syncthreads();
+    // the staged h lives in the A digit area: clear it before the first tile
+    for (int i = tid; i < kOzDigits * Sh::A_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4 *>(Ad)[i] = make_uint4(0, 0, 0, 0);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -161,36 +197,53 @@ __global__ void __launch_bounds__(128) k_sym_gemm_oz(SymDev s, int k)
     const int ntiles = 2 * s.gemm_tiles;
     uint32_t phase = 0;
     bool ok = true;
+    __shared__ int tile_c[Sh::CPT], tile_p[Sh::CPT];
+    constexpr int ITER = Sh::ITER;
     const int sub = lane / Sh::LPR, sl = lane % Sh::LPR;  // row within the warp load, lane within the row
     for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const int t = tile / s.gemm_tiles, g = tile % s.gemm_tiles;
+        if (tid < Sh::CPT) {
+            tile_c[tid] = s.gemm_c[g * Sh::CPT + tid];
+            tile_p[tid] = s.gemm_partner[g * Sh::CPT + tid];
+        }
+        __syncthreads();
         const float *Xg = sym_in(s, k) + t * 2 * s.n4;
-        // A digits: rows m = slot*NN + mu2, 4 floats per lane, row maximum by shuffles
-        for (int base = warp * Sh::RPW; base < 128; base += 4 * Sh::RPW) {
-            const int m = base + sub;
+        // A digits: rows m = slot*NN + mu2; all loads of the tile issued first
+        float4 v[ITER];
+#pragma unroll
+        for (int it = 0; it < ITER; ++it) {
+            const int m = (warp + Sh::WARPS * it) * Sh::RPW + sub;
             const int slot = m / NN, mu2 = m % NN;
-            const int c = s.gemm_c[g * Sh::CPT + slot];
-            const float4 v = reinterpret_cast<const float4 *>(Xg + ((long long)mu2 * n2 + c) * Sh::K)[sl];
-            float mx = fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
+            v[it] = reinterpret_cast<const float4 *>(Xg + ((long long)mu2 * n2 + tile_c[slot]) * Sh::K)[sl];
+        }
+#pragma unroll
+        for (int it = 0; it < ITER; ++it) {
+            const int m = (warp + Sh::WARPS * it) * Sh::RPW + sub;
+            float mx = fmaxf(fmaxf(fabsf(v[it].x), fabsf(v[it].y)), fmaxf(fabsf(v[it].z), fabsf(v[it].w)));
 #pragma unroll
             for (int o = Sh::LPR / 2; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            const int e = (mx > 0.f) ? ilogbf(mx) : 0;
+            // exponent of the row maximum straight from the bits (mx is normal or zero)
+            // (clamped: rows below 2^-100 keep 2^-128 absolute accuracy, far under the state's scale)
+            const int e = (mx > 0.f) ? max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, -100) : 0;
             if (sl == 0) eA[m] = e;
-            const float vv[4] = {v.x, v.y, v.z, v.w};
-            __nv_bfloat16 dq[kOzDigits][4];
+            const float sc = pow2f(20 - e);
+            const float vv[4] = {v[it].x * sc, v[it].y * sc, v[it].z * sc, v[it].w * sc};
+            float d[kOzDigits][4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                float d[kOzDigits];
-                oz_digits(ldexpf(vv[i], 20 - e), d);
+                float dd[kOzDigits];
+                oz_digits(vv[i], dd);
 #pragma unroll
-                for (int q = 0; q < kOzDigits; ++q) dq[q][i] = __float2bfloat16_rn(d[q]);
+                for (int q = 0; q < kOzDigits; ++q) d[q][i] = dd[q];
             }
             const int kk0 = sl * 4;
 #pragma unroll
             for (int q = 0; q < kOzDigits; ++q) {
+                const __nv_bfloat162 lo = __floats2bfloat162_rn(d[q][0], d[q][1]);
+                const __nv_bfloat162 hi = __floats2bfloat162_rn(d[q][2], d[q][3]);
                 uint2 w;
-                w.x = uint32_t(__bfloat16_as_ushort(dq[q][0])) | (uint32_t(__bfloat16_as_ushort(dq[q][1])) << 16);
-                w.y = uint32_t(__bfloat16_as_ushort(dq[q][2])) | (uint32_t(__bfloat16_as_ushort(dq[q][3])) << 16);
+                w.x = *reinterpret_cast<const uint32_t *>(&lo);
+                w.y = *reinterpret_cast<const uint32_t *>(&hi);
                 *reinterpret_cast<uint2 *>(Ad + q * Sh::A_BYTES + swz_byte(m, kk0)) = w;
             }
         }
@@ -220,38 +273,44 @@ __global__ void __launch_bounds__(128) k_sym_gemm_oz(SymDev s, int k)
             break;
         }
         tc_fence_after();
-        // TMEM -> FP64 combination -> FP32 staging S[row][j]
-        const int row = warp * 32 + lane;
-        const double sa = ldexp(1.0, eA[row] - 6);
-#pragma unroll 1
-        for (int cc = 0; cc < Sh::N / 32; ++cc) {
-            double accd[32];
+        // TMEM -> FP64 combination -> FP32 staging S[row][j]; two warps per lane
+        // quadrant, each taking half of the columns
+        {
+            const int quad = warp & 3, half = warp >> 2;
+            const int row = quad * 32 + lane;
+            const double sa = ldexp(1.0, eA[row] - 6);
+            const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + half * Sh::HALF;
+            double acc[Sh::HALF];
 #pragma unroll
-            for (int i = 0; i < 32; ++i) accd[i] = 0.0;
+            for (int i = 0; i < Sh::HALF; ++i) acc[i] = 0.0;
 #pragma unroll
             for (int L = kOzLevels - 1; L >= 0; --L) {
-                float v[32];
-                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + L * Sh::N + cc * 32, v);
-                const double w = ldexp(1.0, -7 * L);
+                float v[Sh::HALF];
+                tmem_ldw<Sh::HALF>(ta + L * Sh::N, v);
+                // sum_L 2^(-7L) P_L, smallest level first
 #pragma unroll
-                for (int i = 0; i < 32; ++i) accd[i] += w * double(v[i]);
+                for (int i = 0; i < Sh::HALF; ++i) acc[i] = acc[i] * 0x1p-7 + double(v[i]);
             }
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const int j = cc * 32 + i;
-                S[row * Sh::S_LD + j] = float(accd[i] * sa * ldexp(1.0, eB[j] - 6));
+            for (int i = 0; i < Sh::HALF; ++i) {
+                const int j = half * Sh::HALF + i;
+                S[row * Sh::S_LD + j] = float(acc[i] * sa * sB[j]);
             }
         }
         tc_fence_before();
         __syncthreads();
+        // W[mu1][mu2][c] = T1[mu1][mu2][c] + T1[mu2][mu1][cbar]; stores run along r
         float *Wg = s.W + t * 2 * s.n4;
-        for (int e = tid; e < Sh::CPT * 2 * NN * NN; e += blockDim.x) {
-            const int r = e % (NN * NN), part = (e / (NN * NN)) % 2, slot = e / (2 * NN * NN);
-            const int mu1 = r % NN, mu2 = r / NN;
-            const int ps = s.gemm_partner[g * Sh::CPT + slot];
-            const float v = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] + S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
-            const int c = s.gemm_c[g * Sh::CPT + slot];
-            Wg[((long long)c * 2 + part) * n2 + r] = v;
+#pragma unroll 1
+        for (int sp = 0; sp < Sh::CPT * 2; ++sp) {
+            const int slot = sp >> 1, part = sp & 1;
+            const int ps = tile_p[slot];
+            float *Wrow = Wg + ((long long)tile_c[slot] * 2 + part) * n2;
+#pragma unroll
+            for (int r = tid; r < NN * NN; r += kOzThreads) {
+                const int mu1 = r % NN, mu2 = r / NN;
+                Wrow[r] = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] + S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
+            }
         }
         // (the staging overwrote the digit buffers; the MMAs read only the K steps
         // the next tile rewrites, so no clearing is needed)

@@ -155,6 +155,27 @@ const char *g12_kernel_name(const g12_ctx *ctx, int32_t kind);
  * FP64 roofline denominator, which the tensor-core peaks do not cover. */
 double g12_fp64_peak_tflops(int32_t device);
 
+/* ---- batched ensembles ---------------------------------------------------
+ * Many independent systems (each with its own g12_params: Ns, Nb, U, t2,
+ * quench, ...) advanced together by the FP64 engine: every RK4 stage is one
+ * launch per kernel kind for the whole ensemble, each step one CUDA graph.
+ * Each system's results equal what a single-system context computes.  The
+ * row/column-mixing tile (matrices per block) is autotuned per n at creation.
+ * No counterpart in the reference (which runs one system per process); the
+ * per-system semantics are those of AS.h:63 / RK_solver.h:64. */
+int g12_batch_create(const g12_params *systems, int32_t nsys, int32_t precision, int32_t device,
+                     g12_batch **out);
+int g12_batch_destroy(g12_batch *b);
+const char *g12_batch_last_error(const g12_batch *b);  /* NULL: last creation error */
+int g12_batch_set_state(g12_batch *b, int32_t i, const double *G1, const double *G2xx, const double *G2xy);
+int g12_batch_get_state(g12_batch *b, int32_t i, double *G1, double *G2xx, double *G2xy);
+/* each system runs its own g12_as_steps() steps; the ensemble takes the maximum */
+int g12_batch_adiabatic_switch(g12_batch *b, int64_t *steps_done);
+/* nsteps RK4 steps of every system; dipole_out (nullable) is nsys x nsteps */
+int g12_batch_propagate(g12_batch *b, int64_t nsteps, double *dipole_out, int64_t *steps_done);
+double g12_batch_last_device_ms(const g12_batch *b);
+int32_t g12_batch_tile(const g12_batch *b, int32_t i);  /* autotuned matrices per block of system i */
+
 /* ---- allocation-free entry point ----------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc:
  * code whose device memory is owned by another allocator (a caching or arena

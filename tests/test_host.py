@@ -170,3 +170,13 @@ def test_writers_match_reference_text(g12):
             os.chdir(cwd)
         for name in ("real_G1.txt", "imag_G1.txt", "dipole.txt"):
             assert open(os.path.join(d, name)).read() == open(os.path.join(mine, name)).read(), name
+
+
+def test_ensemble_generator_is_seeded(g12):
+    a = g12.ensemble_params(16)
+    b = g12.ensemble_params(16)
+    assert [p.as_dict() for p in a] == [p.as_dict() for p in b]
+    for p in a:
+        assert p.Ns in (4, 6, 8, 10, 12) and p.Nb in (1, 2)
+        assert 0.5 <= p.U <= 2.5 and 0.5 <= p.quench_strength <= 3.0 and p.Nq == p.Ns // 3
+        assert p.EHM == 1 and p.v_law == 1 and p.dt == 0.01
