@@ -39,7 +39,20 @@ WORKLOAD = dict(Ns=16, Nb=2, Nq=4, time_steps=10000, U=1.5, t1=1.0, t2=0.3, dt=0
 METRIC = "RK4 steps/s at Ns=16,Nb=2: mixed/learned vs plain FP64 on B200, G1 err<=1e-6"
 CONFIG = {"workload": "HF-GKBA GW, Hubbard chain Ns=16 Nb=2 (n=32), EHM w(r)=U/(1+r), U=1.5, t2=0.3, "
                       "full quench 1.5 on Nq=4, dt=0.01",
-          "n": 32, "g2_entries_per_tensor": 32 ** 4, "l2_policy": "working set 160 MB > 126 MB L2"}
+          "n": 32, "g2_entries_per_tensor": 32 ** 4,
+          "l2_policy": "L2 flushed between steps: every timed step ends with a 160 MiB device write "
+                       "(counted in the timed region); the mixed engine's working set (85 MB) would "
+                       "otherwise stay in the 126 MB L2"}
+EVICT_BYTES = 160 << 20
+
+
+# DRAM bytes (read + write) per launch of the top kernels, from one
+# `ncu --set full` capture each (profiles/ summaries name the command).
+TOP_KERNEL_DRAM_BYTES = {
+    "k_sym_gemm_oz": 16906496.0,
+    "k_sym_epi": 55267328.0,
+    "k_apply<cols+epilogue>": 95704832.0,
+}
 
 
 def log(*a):
@@ -174,14 +187,45 @@ def run_reference_arm(args):
     }))
 
 
+def ensemble_measure(g12, local, steps=20, warmup=3, sample=16):
+    """256 uneven systems (n = 4..24) in one batch (FP64 engine) against the same
+    systems run one context at a time (a seeded sample of them, scaled).  The
+    ensemble's state (about 2 GB) is far larger than L2."""
+    ps = g12.ensemble_params(256)
+    with g12.Batch(ps, "fp64", local) as b:
+        for i, p in enumerate(ps):
+            b.set_state(i, g12.make_G0(p))
+        b.propagate(warmup)
+        b.propagate(steps)
+        ms = b.last_device_ms
+    rng = np.random.default_rng(1)
+    idx = rng.choice(len(ps), size=sample, replace=False)
+    seq_ms = 0.0
+    for i in idx:
+        with g12.Context(ps[i], "fp64", local) as ctx:
+            ctx.set_state(g12.make_G0(ps[i]))
+            ctx.propagate_dipole(warmup)
+            ctx.propagate_dipole(steps)
+            seq_ms += ctx.last_device_ms
+    seq_total = seq_ms * len(ps) / sample
+    ns = [p.n for p in ps]
+    return {"systems": len(ps), "n_values": sorted(set(ns)), "ensemble_steps_per_s": steps / (ms / 1e3),
+            "system_steps_per_s": len(ps) * steps / (ms / 1e3),
+            "one_context_at_a_time_steps_per_s": steps / (seq_total / 1e3),
+            "speedup_vs_one_context_at_a_time": seq_total / ms,
+            "note": f"{steps} timed steps after {warmup}; sequential figure from {sample} sampled systems x "
+                    f"{len(ps)}/{sample}; from G0 with G2 = 0 (step cost does not depend on the state)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32x3", "bf16oz", "tf32x6", "fp32"])
+    ap.add_argument("--precision", default="bf16oz", choices=["fp64", "tf32x3", "bf16oz", "tf32x6", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--skip-as", action="store_true",
                     help="start the timed steps from G0 (profiling runs); the cost of a step does not depend on the state")
     args = ap.parse_args()
@@ -195,67 +239,99 @@ def main():
     p = g12.make_params(**WORKLOAD)
     n = p.n
     G0 = g12.make_G0(p)
+    K = args.steps
 
-    # prepared state: adiabatic switching (untimed), then the timed RK4 steps
-    def prepared(prec):
-        ctx = g12.Context(p, prec, local)
-        ctx.set_state(G0)
-        if not args.skip_as:
-            ctx.adiabatic_switch()
-        return ctx
+    # plain FP64 path: prepared state S (adiabatic switching, untimed)
+    fp = g12.Context(p, "fp64", local)
+    fp.set_state(G0)
+    if not args.skip_as:
+        fp.adiabatic_switch()
+    S = fp.get_state()
+    fp.propagate_dipole(args.warmup)
+    mixed = args.precision != "fp64"
+    mx = g12.Context(p, args.precision, local) if mixed else fp
+    if mixed:
+        mx.set_state(*S)
+        mx.propagate_dipole(args.warmup)
 
-    ctx = prepared(args.precision)
-    state = ctx.get_state()
-    ctx.propagate_dipole(args.warmup)
+    # timed: K RK4 steps from S on each path (device time, CUDA events).  Every
+    # step ends with a write of EVICT_BYTES (> L2) inside the timed region, so
+    # the next step finds its state in HBM, not L2.
+    for c in {id(fp): fp, id(mx): mx}.values():
+        c.set_l2_eviction(EVICT_BYTES)
     barrier(pg)
+    fp.set_state(*S)
+    traj_fp, rc_fp = fp.propagate(K)
+    ms_fp = allmax(pg, fp.last_device_ms)
+    barrier(pg)
+    mx.set_state(*S)
     with Clocks(local) as clk:
-        _, rc = ctx.propagate_dipole(args.steps)
-        dev_ms = ctx.last_device_ms
+        traj_mx, rc = mx.propagate(K)
+        dev_ms = mx.last_device_ms
     barrier(pg)
     ms = allmax(pg, dev_ms)
-    value = world * args.steps / (ms / 1e3)
-    launches = ctx.launches_per_step * args.steps
+    # the same steps without the eviction write (state L2-resident between steps)
+    mx.set_l2_eviction(0)
+    mx.set_state(*S)
+    mx.propagate_dipole(K)
+    ms_res = allmax(pg, mx.last_device_ms)
+    mx.set_l2_eviction(EVICT_BYTES)
+    value = world * K / (ms / 1e3)
+    value_fp = world * K / (ms_fp / 1e3)
+    g1_err = float(np.max(np.abs(traj_mx - traj_fp)) / np.max(np.abs(traj_fp)))
+    launches = mx.launches_per_step * K
 
-    # e2e through the C ABI with host buffers
-    traj_host = np.zeros((args.steps, n, n), np.complex128)
+    # e2e through the C ABI with host buffers (headline path, eviction on)
+    import ctypes
+    traj_host = np.zeros((K, n, n), np.complex128)
+    done = ctypes.c_int64()
     barrier(pg)
     t0 = time.perf_counter()
-    ctx.set_state(*state)
-    t_mid = time.perf_counter()
-    import ctypes
-    done = ctypes.c_int64()
-    g12.lib().g12_propagate(ctx.h, args.steps, traj_host.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                            ctypes.byref(done))
-    out = ctx.get_state()
+    mx.set_state(*S)
+    g12.lib().g12_propagate(mx.h, K, traj_host.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(done))
+    mx.get_state()
     t1 = time.perf_counter()
     e2e_s = allmax(pg, t1 - t0)
     state_bytes = (n * n + 2 * n ** 4) * 16
-    e2e = {"value": world * args.steps / e2e_s, "unit": "steps/s",
-           "h2d_bytes_per_step": state_bytes / args.steps,
-           "d2h_bytes_per_step": n * n * 16 + state_bytes / args.steps,
+    e2e = {"value": world * K / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": state_bytes / K,
+           "d2h_bytes_per_step": n * n * 16 + state_bytes / K,
            "note": "set_state + propagate(K, per-step G1 snapshots to host) + get_state, wall clock"}
 
-    # per-kernel device times (CUDA events on the library stream), roofline of the top kernel
-    kt = ctx.kernel_times(2)
-    ctx.close()
+    # per-kernel device times (CUDA events around each launch on the library stream)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0, "source": "fallback"}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    kt = mx.kernel_times(2)
     tot = sum(a * c for a, c in kt.values())
+    kernels = {k: {"ms_per_launch": a, "launches_per_step": c, "share": a * c / tot} for k, (a, c) in kt.items()}
     top = max(kt, key=lambda k: kt[k][0] * kt[k][1])
     top_ms = kt[top][0]
     fp64_peak = g12.fp64_peak_tflops(local)
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
-    # one k_apply launch: both tensors, one stage, two of the four mode products:
-    # 2 * 2 * n^5 complex MACs * 8 flops; algorithmic bytes: half of the stage's
-    # 5 state passes over 2 tensors (640 n^4 B per step / 8 apply launches)
-    flops = 32.0 * n ** 5
-    bytes_alg = 80.0 * n ** 4
-    roofline = {"bound": "fp64", "kernel": top, "achieved": flops / (top_ms * 1e-3) / 1e12,
-                "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": flops / (top_ms * 1e-3) / 1e12 / fp64_peak, "traffic": None,
-                "peak_source": "measured FP64 FMA probe (g12_fp64_peak_tflops) on this GPU",
-                "hbm_achieved_gbs": bytes_alg / (top_ms * 1e-3) / 1e9, "hbm_peak_gbs": peaks.get("hbm_gbs"),
-                "hbm_frac": bytes_alg / (top_ms * 1e-3) / 1e9 / peaks.get("hbm_gbs", 6650.0)}
-    kernels = {k: {"ms_per_launch": a, "launches_per_step": c, "share": a * c / tot} for k, (a, c) in kt.items()}
+    if mixed:
+        # k_sym_gemm_*: reads the FP32 stage input, writes W (FP32), both tensors:
+        # 2 x n^4 x (8 + 8) bytes per launch
+        bytes_alg = 32.0 * n ** 4 if "gemm" in top else 40.0 * n ** 4
+        roofline = {"bound": "hbm", "kernel": top, "achieved": bytes_alg / (top_ms * 1e-3) / 1e9, "peak": hbm,
+                    "unit": "GB/s", "frac": bytes_alg / (top_ms * 1e-3) / 1e9 / hbm,
+                    "traffic": TOP_KERNEL_DRAM_BYTES.get(top), "algorithmic_bytes": bytes_alg,
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "source" not in peaks else "fallback"}
+    else:
+        flops = 32.0 * n ** 5
+        roofline = {"bound": "fp64", "kernel": top, "achieved": flops / (top_ms * 1e-3) / 1e12, "peak": fp64_peak,
+                    "unit": "TFLOP/s", "frac": flops / (top_ms * 1e-3) / 1e12 / fp64_peak,
+                    "traffic": TOP_KERNEL_DRAM_BYTES.get(top),
+                    "peak_source": "measured FP64 FMA probe (g12_fp64_peak_tflops) on this GPU"}
+    # whole step against the per-step figure 640 n^4 bytes (FP64 state passes)
+    step_roofline = {"bytes_per_step": 640.0 * n ** 4, "achieved_gbs": 640.0 * n ** 4 * value / world / 1e9,
+                     "frac_of_hbm": 640.0 * n ** 4 * value / world / 1e9 / hbm,
+                     "flops_per_step": 256.0 * n ** 5, "fp64_peak_tflops": fp64_peak}
+    if mixed:
+        mx.close()
+    fp.close()
+
+    ensemble = None
+    if rank == 0 and not args.no_ensemble:
+        ensemble = ensemble_measure(g12, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -266,13 +342,19 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else args.precision,
+            "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if not mixed else args.precision,
             "data": "synthetic (physics-defined input: make_G0 + adiabatic switching)",
             "config": dict(CONFIG, precision=args.precision, parallelism=f"replicas x{world}"),
-            "status": rc, "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "kernels": kernels,
-            "cpu_baseline": cpu, "clocks": clk.summary(),
+            "status": rc, "l2_resident": {"value": world * K / (ms_res / 1e3), "unit": "steps/s",
+                                          "ms_per_step": ms_res / K},
+            "plain_fp64": {"value": value_fp, "unit": "steps/s", "ms_per_step": ms_fp / K,
+                                         "status": rc_fp},
+            "speedup_vs_plain_fp64": value / value_fp,
+            "g1_max_rel_err_vs_fp64": g1_err,
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline,
+            "kernels": kernels, "ensemble": ensemble, "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line))
     if pg is not None:

@@ -103,6 +103,8 @@ def lib():
         L.g12_kernel_times.argtypes = [C.c_void_p, C.c_int32, _dp, C.POINTER(C.c_int32), C.c_int32]
         L.g12_kernel_name.restype = C.c_char_p
         L.g12_kernel_name.argtypes = [C.c_void_p, C.c_int32]
+        L.g12_set_l2_eviction.restype = C.c_int32
+        L.g12_set_l2_eviction.argtypes = [C.c_void_p, C.c_int64]
         L.g12_fp64_peak_tflops.restype = C.c_double
         L.g12_fp64_peak_tflops.argtypes = [C.c_int32]
         L.g12_batch_create.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
@@ -284,6 +286,11 @@ class Context:
     @property
     def launches_per_step(self) -> int:
         return int(lib().g12_launches_per_step(self.h))
+
+    def set_l2_eviction(self, nbytes):
+        """Write ``nbytes`` of a scratch buffer after every step (0 = off), so
+        each step starts with the state evicted from L2."""
+        _check(lib().g12_set_l2_eviction(self.h, int(nbytes)), self.h)
 
     def kernel_times(self, nsteps=2):
         """{kernel name: (mean ms per launch, launches per step)} measured with

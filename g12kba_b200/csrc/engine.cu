@@ -54,6 +54,8 @@ struct g12_ctx {
     double t_rk = 0, t_temp = 0;   // RK4 clock (RK_solver.h:78-80)
     float last_ms = 0;
     std::vector<void *> allocs;
+    void *evict_buf = nullptr;      // g12_set_l2_eviction: written after every step
+    size_t evict_bytes = 0;
 };
 
 namespace {
@@ -225,6 +227,7 @@ void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
         }
         cudaStreamWaitEvent(s, ctx->ev_join, 0);
     }
+    if (ctx->evict_bytes) cudaMemsetAsync(ctx->evict_buf, 0, ctx->evict_bytes, s);
 }
 
 int build_graph(g12_ctx *ctx)
@@ -417,6 +420,7 @@ extern "C" int g12_destroy(g12_ctx *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->s) cudaStreamSynchronize(ctx->s);
     if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+    if (ctx->evict_buf) cudaFree(ctx->evict_buf);
     mixed_free(ctx->mixed);
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->sched_dev) cudaFree(ctx->sched_dev);
@@ -612,6 +616,29 @@ extern "C" int g12_rhs(g12_ctx *ctx, const double *G1, const double *G2xx, const
 
 extern "C" double g12_last_device_ms(const g12_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
 
+extern "C" int32_t g12_set_l2_eviction(g12_ctx *ctx, int64_t bytes)
+{
+    if (!ctx || bytes < 0) return G12_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->s));
+    if (ctx->graph) {
+        cudaGraphExecDestroy(ctx->graph);
+        ctx->graph = nullptr;
+    }
+    if (ctx->evict_buf) cudaFree(ctx->evict_buf);
+    ctx->evict_buf = nullptr;
+    ctx->evict_bytes = 0;
+    if (bytes == 0) return G12_OK;
+    if (cudaMalloc(&ctx->evict_buf, size_t(bytes)) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->evict_buf = nullptr;
+        ctx->err = "out of device memory (L2 eviction buffer)";
+        return G12_ERR_NOMEM;
+    }
+    ctx->evict_bytes = size_t(bytes);
+    return G12_OK;
+}
+
 namespace {
 
 const char *kFp64Names[] = {"k_step_begin", "k_prep", "k_g1", "k_apply<rows>", "k_apply<cols+epilogue>"};
@@ -673,6 +700,7 @@ extern "C" int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms
                     timed(3 + q, [&] { mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, q, ctx->s); });
             }
         }
+        if (ctx->evict_bytes) cudaMemsetAsync(ctx->evict_buf, 0, ctx->evict_bytes, ctx->s);
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);

@@ -151,6 +151,14 @@ int32_t g12_launches_per_step(const g12_ctx *ctx);
 int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms, int32_t *calls_per_step, int32_t cap);
 const char *g12_kernel_name(const g12_ctx *ctx, int32_t kind);
 
+/* Measurement aid: after every RK4 step (in g12_propagate*, g12_adiabatic_switch
+ * and g12_kernel_times) write `bytes` bytes of a private device buffer, so that
+ * every step starts with the state evicted from L2 (126 MB on B200), as it
+ * would if the working set exceeded L2.  The write is extra work inside
+ * the step, never skipped work.  0 (the default) switches it off.  No
+ * counterpart in the reference. */
+int32_t g12_set_l2_eviction(g12_ctx *ctx, int64_t bytes);
+
 /* Measured FP64 FMA throughput of `device` (TFLOP/s, 2 flops per FMA): the
  * FP64 roofline denominator, which the tensor-core peaks do not cover. */
 double g12_fp64_peak_tflops(int32_t device);

@@ -83,3 +83,20 @@ def test_mixed_state_roundtrip_keeps_symmetry(g12):
         g1, xx, xy = ctx.get_state()
     assert np.array_equal(g1, G1.astype(complex))
     assert rel_err(xx, XX) <= 1e-15 and rel_err(xy, XY) <= 1e-15
+
+
+@pytest.mark.parametrize("prec", ["fp64", "bf16oz"])
+def test_l2_eviction_changes_nothing(g12, prec):
+    p = g12.make_params(Ns=8, Nb=2, Nq=2, U=1.5, t2=0.3, EHM=True, v_law="inv", dt=0.01)
+    G1, XX, XY = physical_state(np.random.default_rng(3), 8, 2)
+    out = []
+    for evict in (0, 160 << 20):
+        with g12.Context(p, prec) as ctx:
+            ctx.set_l2_eviction(evict)
+            ctx.set_state(G1, XX, XY)
+            traj, rc = ctx.propagate(5)
+            assert rc == 0
+            out.append((traj, ctx.get_state()))
+    assert np.array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1], out[1][1]):
+        assert np.array_equal(a, b)
