@@ -122,6 +122,25 @@ def lib():
         L.g12_rhs_noalloc.argtypes = [C.POINTER(Params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                       C.c_double, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_char_p, C.c_int32]
+        _vp, _fp, _i64p = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_int64)
+        L.g12_batch_propagate_features.argtypes = [_vp, C.c_int64, C.c_int32, _vp, _dp, _i64p]
+        L.g12_mlp_create.argtypes = [C.POINTER(C.c_int32), C.c_int32, C.c_uint64, C.c_int32, C.POINTER(C.c_void_p)]
+        L.g12_mlp_destroy.argtypes = [_vp]
+        L.g12_mlp_last_error.restype = C.c_char_p
+        L.g12_mlp_last_error.argtypes = [_vp]
+        L.g12_mlp_param_count.restype = C.c_int64
+        L.g12_mlp_param_count.argtypes = [_vp]
+        L.g12_mlp_set_params.argtypes = [_vp, _fp]
+        L.g12_mlp_get_params.argtypes = [_vp, _fp]
+        L.g12_mlp_get_grads.argtypes = [_vp, _fp]
+        L.g12_mlp_forward.argtypes = [_vp, _vp, C.c_int32, _vp]
+        L.g12_mlp_loss_grad.argtypes = [_vp, _vp, _vp, C.c_int32, _dp]
+        L.g12_mlp_adam.argtypes = [_vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]
+        L.g12_mlp_set_norm.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int32, _fp, C.c_float, C.c_float, C.c_float]
+        L.g12_mlp_windows.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, _vp, _vp]
+        L.g12_mlp_train_windows.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, C.c_float, C.c_float,
+                                            _dp]
+        L.g12_mlp_rollout.argtypes = [_vp, _vp, C.c_int32, C.c_int64, C.c_int64, _fp]
         _lib = L
     return _lib
 
@@ -361,6 +380,17 @@ class Batch:
         dip = np.zeros((self.nsys, max(nsteps, 1)))
         done = C.c_int64()
         self._chk(lib().g12_batch_propagate(self.h, nsteps, _ptr(dip), C.byref(done)))
+        return dip[:, :nsteps]
+
+    def propagate_features(self, nsteps, every, feat_ptr):
+        """nsteps RK4 steps recording snapshot features (rho = -i G1, upper
+        triangle, real then imaginary parts) every `every` steps into the device
+        buffer at feat_ptr [nsys][nsteps // every][n(n+1)] (float32); returns
+        the dipoles (nsys, nsteps)."""
+        dip = np.zeros((self.nsys, max(nsteps, 1)))
+        done = C.c_int64()
+        self._chk(lib().g12_batch_propagate_features(self.h, nsteps, every, C.c_void_p(feat_ptr), _ptr(dip),
+                                                     C.byref(done)))
         return dip[:, :nsteps]
 
     @property

@@ -113,6 +113,27 @@ __global__ void kb_gather_dip(BatchDev b, int steps, double *out)
         out[(long long)i * steps + s] = d.dip[s % d.dip_cap];
 }
 
+// snapshot features of every system (state after the step just run):
+// rho = -i G1, upper triangle (mu <= nu, row-major), real parts then imaginary
+// parts -> feat[sys][snap][n(n+1)]
+__global__ void kb_features(BatchDev b, long long snap, long long nsnap, float *feat)
+{
+    const int i = blockIdx.y;
+    const Dev &d = b.devs[i];
+    const int n = d.n, nt = n * (n + 1) / 2;
+    float *out = feat + ((long long)i * nsnap + snap) * (2 * nt);
+    for (int x = threadIdx.x; x < nt; x += blockDim.x) {
+        int mu = 0, r = x;
+        while (r >= n - mu) {
+            r -= n - mu;
+            ++mu;
+        }
+        const double2 g = d.Y1[mu * n + mu + r];
+        out[x] = float(g.y);
+        out[nt + x] = float(-g.x);
+    }
+}
+
 ApplyCfg apply_cfg_nb(int n, int nb)
 {
     ApplyCfg c;
@@ -339,9 +360,10 @@ int build_batch_graph(g12_batch *b)
     return G12_OK;
 }
 
-// runs `steps` steps of each system's schedule (filled chunk by chunk by `fill`)
-template <typename Fill>
-int batch_run(g12_batch *b, long long steps, double *dip_out, Fill fill)
+// runs `steps` steps of each system's schedule (filled chunk by chunk by
+// `fill`); after(step) may enqueue work after each step's graph
+template <typename Fill, typename After>
+int batch_run(g12_batch *b, long long steps, double *dip_out, Fill fill, After after)
 {
     int rc = build_batch_graph(b);
     if (rc) return rc;
@@ -355,7 +377,11 @@ int batch_run(g12_batch *b, long long steps, double *dip_out, Fill fill)
         if (rc) return rc;
         BCK(cudaStreamSynchronize(b->s));
         BCK(cudaEventRecord(b->ev0, b->s));
-        for (long long q = 0; q < n; ++q) BCK(cudaGraphLaunch(b->graph, b->s));
+        for (long long q = 0; q < n; ++q) {
+            BCK(cudaGraphLaunch(b->graph, b->s));
+            after(base + q);
+        }
+        BCK(cudaGetLastError());
         BCK(cudaEventRecord(b->ev1, b->s));
         BCK(cudaStreamSynchronize(b->s));
         float ms = 0;
@@ -633,10 +659,39 @@ extern "C" int g12_batch_propagate(g12_batch *b, int64_t nsteps, double *dipole_
 {
     if (!b || nsteps < 0) return G12_ERR_INVALID;
     BCK(cudaSetDevice(b->device));
-    int rc = batch_run(b, nsteps, dipole_out, [&](long long, long long n) {
-        for (int i = 0; i < b->nsys; ++i)
-            rk_sched(b->P[i], n, &b->t_rk[i], &b->t_temp[i], b->sched_h + size_t(i) * kChunk);
-    });
+    int rc = batch_run(
+        b, nsteps, dipole_out,
+        [&](long long, long long n) {
+            for (int i = 0; i < b->nsys; ++i)
+                rk_sched(b->P[i], n, &b->t_rk[i], &b->t_temp[i], b->sched_h + size_t(i) * kChunk);
+        },
+        [](long long) {});
+    if (steps_done) *steps_done = rc == G12_OK ? nsteps : 0;
+    return rc;
+}
+
+extern "C" int g12_batch_propagate_features(g12_batch *b, int64_t nsteps, int32_t every, float *feat_dev,
+                                            double *dipole_out, int64_t *steps_done)
+{
+    if (!b || nsteps < 0 || every < 1 || !feat_dev) return G12_ERR_INVALID;
+    const int n = b->P[0].Ns * b->P[0].Nb;
+    for (int i = 1; i < b->nsys; ++i)
+        if (b->P[i].Ns * b->P[i].Nb != n) {
+            b->err = "feature recording needs one n for all systems";
+            return G12_ERR_INVALID;
+        }
+    BCK(cudaSetDevice(b->device));
+    const long long nsnap = nsteps / every;
+    int rc = batch_run(
+        b, nsteps, dipole_out,
+        [&](long long, long long nn) {
+            for (int i = 0; i < b->nsys; ++i)
+                rk_sched(b->P[i], nn, &b->t_rk[i], &b->t_temp[i], b->sched_h + size_t(i) * kChunk);
+        },
+        [&](long long step) {
+            if ((step + 1) % every == 0 && (step + 1) / every <= nsnap)
+                kb_features<<<dim3(1, b->nsys), 128, 0, b->s>>>(b->bd, (step + 1) / every - 1, nsnap, feat_dev);
+        });
     if (steps_done) *steps_done = rc == G12_OK ? nsteps : 0;
     return rc;
 }

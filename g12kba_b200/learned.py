@@ -1,0 +1,266 @@
+"""Learned G1 extrapolator: a network trained on trajectories that the
+propagation engine generates, mapping a window of K past G1 snapshots to the
+next M snapshots.  No counterpart in the reference (G12KBA-GW has no learned
+component); the RK4 propagation stays the judge of its error and the fallback.
+
+Training, inference and data generation all run on the GPU through the C ABI
+(``g12_mlp_*``, ``g12_batch_propagate_features``); torch only provides device
+buffers.  Snapshots are spaced ``stride`` RK4 steps apart.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import Batch, Context, G12Error, dipole, lib, make_G0, make_params
+
+DEFAULT_DIMS = (8704, 512, 512, 512, 4352)
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def features(G1):
+    """rho = -i G1 [..., n, n] -> upper triangle (mu <= nu, row-major), real
+    parts then imaginary parts (float32), the layout the kernels use."""
+    G1 = np.asarray(G1)
+    n = G1.shape[-1]
+    iu = np.triu_indices(n)
+    rho = -1j * G1[..., iu[0], iu[1]]
+    return np.concatenate([rho.real, rho.imag], axis=-1).astype(np.float32)
+
+
+def g1_from_features(f, n):
+    """Inverse of features(): G1 = i rho with rho Hermitian."""
+    f = np.asarray(f, np.float64)
+    nt = n * (n + 1) // 2
+    iu = np.triu_indices(n)
+    rho = np.zeros(f.shape[:-1] + (n, n), np.complex128)
+    rho[..., iu[0], iu[1]] = f[..., :nt] + 1j * f[..., nt:]
+    rho = rho + np.conj(np.swapaxes(rho, -1, -2)) - np.eye(n) * np.real(rho[..., np.arange(n), np.arange(n)])[..., None]
+    return 1j * rho
+
+
+def dipole_from_features(f, n):
+    """dipole.h:25-32 from features (Im G1_ii = Re rho_ii)."""
+    f = np.asarray(f, np.float64)
+    diag = np.array([i * n - i * (i - 1) // 2 for i in range(n)])
+    d = f[..., diag]
+    p = np.zeros(f.shape[:-1])
+    for i in range(n // 2):
+        p += 2.0 * (n / 2.0 - i - 0.5) * (d[..., i] - d[..., n - 1 - i]) / n
+    return p
+
+
+def window_params(nsys, seed, time_steps=6000, Ns=8, Nb=2):
+    """The learned-extrapolator family: Ns=8, Nb=2 (n=16), t1=1, t2=0.5, EHM
+    w(r)=U/(1+r), U ~ U[1,3], full quench of strength ~ U[0.5,3] on Nq=3 sites,
+    dt=0.01.  The quench is switched on at t=1 (quench_gate 0, rate 0.2) so that
+    the trajectories hold post-quench dynamics from their start."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    out = []
+    for _ in range(nsys):
+        U = float(rng.uniform(1.0, 3.0))
+        qs = float(rng.uniform(0.5, 3.0))
+        out.append(make_params(Ns=Ns, Nb=Nb, Nq=3, U=U, t1=1.0, t2=0.5, EHM=True, v_law="inv", dt=0.01,
+                               time_steps=time_steps, q_type="full", quench_strength=qs, quench_gate=0.0,
+                               quench_on_midpoint=1.0, quench_rate=0.2))
+    return out
+
+
+def generate(params, nsteps, stride=1, device=0):
+    """Trajectories of every system (G0, adiabatic switching, nsteps RK4 steps)
+    as snapshot features on the device: torch float32 [nsys][nsteps//stride][F],
+    plus the per-step dipoles (numpy) and the device milliseconds."""
+    torch = _torch()
+    n = params[0].n
+    F = n * (n + 1)
+    snaps = nsteps // stride
+    feat = torch.zeros((len(params), snaps, F), dtype=torch.float32, device=f"cuda:{device}")
+    torch.cuda.synchronize()
+    with Batch(params, "fp64", device) as b:
+        for i, p in enumerate(params):
+            b.set_state(i, make_G0(p))
+        b.adiabatic_switch()
+        dip = b.propagate_features(nsteps, stride, feat.data_ptr())
+        ms = b.last_device_ms
+    return feat, dip, ms
+
+
+def stable(feat, bound=1.5):
+    """Trajectories that stay finite with every density below `bound` (the
+    reference's density guard, RK_solver.h:101-110, stops a run once
+    2 Im G1_00 > 3); torch bool [ntraj]."""
+    torch = _torch()
+    return torch.isfinite(feat).all(dim=2).all(dim=1) & (feat.abs().amax(dim=(1, 2)) < bound)
+
+
+class MLP:
+    """The network (``g12_mlp``): FP32 master weights, bf16 tcgen05 GEMMs with
+    FP32 accumulation, Adam."""
+
+    def __init__(self, dims=DEFAULT_DIMS, max_batch=512, seed=0, device=0):
+        self.dims = tuple(int(d) for d in dims)
+        self.max_batch = max_batch
+        self.device = device
+        d = (C.c_int32 * 5)(*self.dims)
+        h = C.c_void_p()
+        rc = lib().g12_mlp_create(d, max_batch, seed, device, C.byref(h))
+        if rc:
+            raise G12Error(f"g12_mlp_create failed ({rc}): {lib().g12_mlp_last_error(None).decode()}")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().g12_mlp_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc):
+        if rc:
+            raise G12Error(f"libg12kba MLP error {rc}: {lib().g12_mlp_last_error(self.h).decode()}")
+
+    @property
+    def param_count(self):
+        return int(lib().g12_mlp_param_count(self.h))
+
+    def get_params(self):
+        out = np.zeros(self.param_count, np.float32)
+        self._chk(lib().g12_mlp_get_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def set_params(self, params):
+        params = np.ascontiguousarray(params, np.float32)
+        assert params.size == self.param_count
+        self._chk(lib().g12_mlp_set_params(self.h, params.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def grads(self):
+        out = np.zeros(self.param_count, np.float32)
+        self._chk(lib().g12_mlp_get_grads(self.h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def forward(self, X):
+        """X: torch float32 (batch, dims[0]) on the device -> (batch, dims[4])."""
+        torch = _torch()
+        Y = torch.empty((X.shape[0], self.dims[4]), dtype=torch.float32, device=X.device)
+        torch.cuda.synchronize()
+        self._chk(lib().g12_mlp_forward(self.h, C.c_void_p(X.data_ptr()), X.shape[0], C.c_void_p(Y.data_ptr())))
+        return Y
+
+    def loss_grad(self, X, Y):
+        _torch().cuda.synchronize()
+        loss = C.c_double()
+        self._chk(lib().g12_mlp_loss_grad(self.h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), X.shape[0],
+                                          C.byref(loss)))
+        return loss.value
+
+    def adam(self, lr, beta1=0.9, beta2=0.999, eps=1e-8, weight_decay=0.0):
+        self._chk(lib().g12_mlp_adam(self.h, lr, beta1, beta2, eps, weight_decay))
+
+    def set_norm(self, K, M, F, mean, s_in, s_abs, s_out):
+        mean = np.ascontiguousarray(mean, np.float32)
+        self._chk(lib().g12_mlp_set_norm(self.h, K, M, F, mean.ctypes.data_as(C.POINTER(C.c_float)), s_in, s_abs,
+                                         s_out))
+
+    def windows(self, feat, idx):
+        torch = _torch()
+        idx = np.ascontiguousarray(idx, np.int64)
+        B = idx.shape[0]
+        X = torch.zeros((B, self.dims[0]), dtype=torch.float32, device=feat.device)
+        Y = torch.zeros((B, self.dims[4]), dtype=torch.float32, device=feat.device)
+        torch.cuda.synchronize()
+        self._chk(lib().g12_mlp_windows(self.h, C.c_void_p(feat.data_ptr()), feat.shape[0], feat.shape[1],
+                                        idx.ctypes.data_as(C.POINTER(C.c_int64)), B, C.c_void_p(X.data_ptr()),
+                                        C.c_void_p(Y.data_ptr())))
+        return X, Y
+
+    def train_windows(self, feat, idx, lr, weight_decay=0.0):
+        idx = np.ascontiguousarray(idx, np.int64)
+        loss = C.c_double()
+        self._chk(lib().g12_mlp_train_windows(self.h, C.c_void_p(feat.data_ptr()), feat.shape[0], feat.shape[1],
+                                              idx.ctypes.data_as(C.POINTER(C.c_int64)), idx.shape[0], lr,
+                                              weight_decay, C.byref(loss)))
+        return loss.value
+
+    def rollout(self, feat, t0):
+        """Fill snapshots t0+1.. of every trajectory of feat (in place); device ms."""
+        _torch().cuda.synchronize()
+        ms = C.c_float()
+        self._chk(lib().g12_mlp_rollout(self.h, C.c_void_p(feat.data_ptr()), feat.shape[0], feat.shape[1], t0,
+                                        C.byref(ms)))
+        return ms.value
+
+
+class Extrapolator:
+    """Window-to-future map over snapshot features: normalisation, training on
+    device trajectories, rollout."""
+
+    def __init__(self, n, K=32, M=16, width=512, max_batch=512, seed=0, device=0):
+        self.n, self.K, self.M = n, K, M
+        self.F = n * (n + 1)
+        self.mlp = MLP((K * self.F, width, width, width, M * self.F), max_batch=max_batch, seed=seed, device=device)
+        self.norm = None
+
+    def fit_norm(self, feat, t_min=0):
+        """Scales from the training trajectories: s_in / s_out = RMS of the
+        window offsets / future offsets, s_abs = RMS deviation from the mean."""
+        torch = _torch()
+        f = feat[:, t_min:].double()
+        mean = f.mean(dim=(0, 1))
+        s_abs = float(torch.sqrt(((f - mean) ** 2).mean()))
+        d_in = f[:, :-(self.K - 1)] - f[:, self.K - 1:]
+        s_in = float(torch.sqrt((d_in ** 2).mean()))
+        d_out = f[:, self.M:] - f[:, :-self.M]
+        s_out = float(torch.sqrt((d_out ** 2).mean()))
+        self.norm = (mean.float().cpu().numpy(), max(s_in, 1e-6), max(s_abs, 1e-6), max(s_out, 1e-6))
+        self.mlp.set_norm(self.K, self.M, self.F, self.norm[0], self.norm[1], self.norm[2], self.norm[3])
+
+    def train(self, feat, steps, batch=512, lr=1e-3, lr_min=1e-5, weight_decay=0.0, t_min=0, seed=0, log=None):
+        """Adam on random windows (cosine learning-rate decay); returns the loss
+        history (one value per step)."""
+        if self.norm is None:
+            self.fit_norm(feat, t_min)
+        rng = np.random.default_rng(seed)
+        ntraj, snaps = feat.shape[0], feat.shape[1]
+        lo = max(self.K - 1, t_min)
+        hi = snaps - self.M  # t + M < snaps
+        hist = []
+        for it in range(steps):
+            idx = np.stack([rng.integers(0, ntraj, batch), rng.integers(lo, hi, batch)], axis=1)
+            a = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * it / max(1, steps)))
+            hist.append(self.mlp.train_windows(feat, idx, a, weight_decay))
+            if log and (it % max(1, steps // 20) == 0 or it == steps - 1):
+                log(f"step {it} lr {a:.2e} loss {hist[-1]:.3e}")
+        return np.array(hist)
+
+    def rollout(self, prefix, total):
+        """prefix: torch float32 [ntraj][t0+1][F] of exact snapshots; returns
+        ([ntraj][total][F] with snapshots t0+1.. predicted, device ms)."""
+        torch = _torch()
+        t0 = prefix.shape[1] - 1
+        total = t0 + 1 + (total - t0 - 1) // self.M * self.M
+        feat = torch.zeros((prefix.shape[0], total, self.F), dtype=torch.float32, device=prefix.device)
+        feat[:, : t0 + 1] = prefix
+        ms = self.mlp.rollout(feat, t0)
+        return feat, ms
+
+
+def dipole_error(p, p_ref):
+    """max_t |p - p_ref| / max(max_t |p_ref|, 1e-12) (the metric's definition)."""
+    return float(np.max(np.abs(p - p_ref)) / max(np.max(np.abs(p_ref)), 1e-12))

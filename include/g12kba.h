@@ -204,6 +204,48 @@ int g12_rhs_noalloc(const g12_params *p, const double *G1_dev, const double *G2x
                     double *K1_dev, double *K2xx_dev, double *K2xy_dev, void *stream,
                     char *err, int32_t errcap);
 
+/* ---- learned G1 extrapolator ---------------------------------------------
+ * No counterpart in the reference (it has no learned component).  An MLP
+ * dims[0] -> dims[1] -> dims[2] -> dims[3] -> dims[4] (GELU after the first
+ * three layers) maps a window of K past G1 snapshots to the next M snapshots.
+ * Snapshot features: rho = -i G1, upper triangle (mu <= nu, row-major), the
+ * n(n+1)/2 real parts then the imaginary parts: F = n(n+1) floats.
+ * Input slots k < K-1 hold (x_{t-K+1+k} - x_t)/s_in, slot K-1 (x_t - mean)/s_abs;
+ * outputs are (x_{t+1+m} - x_t)/s_out.  Weights are FP32 masters rounded to
+ * bf16 in every tcgen05 GEMM (FP32 accumulation); training is Adam on MSE.
+ * Widths must be multiples of 128; batches multiples of 128 (rollouts pad).
+ * Pointers named *_dev are device memory; everything else is host memory. */
+typedef struct g12_mlp g12_mlp;
+int g12_mlp_create(const int32_t *dims, int32_t max_batch, uint64_t seed, int32_t device, g12_mlp **out);
+int g12_mlp_destroy(g12_mlp *m);
+const char *g12_mlp_last_error(const g12_mlp *m);  /* NULL: last creation error */
+int64_t g12_mlp_param_count(const g12_mlp *m);
+/* parameters / gradients, per layer W ([out][in]) then b, FP32 */
+int g12_mlp_set_params(g12_mlp *m, const float *params);
+int g12_mlp_get_params(g12_mlp *m, float *params);
+int g12_mlp_get_grads(g12_mlp *m, float *grads);
+int g12_mlp_forward(g12_mlp *m, const float *X_dev, int32_t batch, float *Y_dev);
+/* mean squared error of forward(X) against Y and all parameter gradients */
+int g12_mlp_loss_grad(g12_mlp *m, const float *X_dev, const float *Y_dev, int32_t batch, double *loss);
+int g12_mlp_adam(g12_mlp *m, float lr, float beta1, float beta2, float eps, float weight_decay);
+int g12_mlp_set_norm(g12_mlp *m, int32_t K, int32_t M, int32_t F, const float *mean, float s_in, float s_abs,
+                     float s_out);
+/* windows of feat_dev [ntraj][snaps][F]: idx = batch pairs (trajectory, t),
+ * t the window's last snapshot (K-1 <= t, t+M < snaps) */
+int g12_mlp_windows(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t snaps, const int64_t *idx,
+                    int32_t batch, float *X_dev, float *Y_dev);
+int g12_mlp_train_windows(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t snaps, const int64_t *idx,
+                          int32_t batch, float lr, float weight_decay, double *loss);
+/* in place: snapshots t0+1 .. snaps-1 of every trajectory from blocks of M
+ * predictions ((snaps-1-t0) % M == 0); device time in *elapsed_ms */
+int g12_mlp_rollout(g12_mlp *m, float *feat_dev, int32_t ntraj, int64_t snaps, int64_t t0, float *elapsed_ms);
+
+/* Batched propagation recording snapshot features (the layout above) of every
+ * system after every `every`-th step into feat_dev [nsys][nsteps/every][F]
+ * (device memory); all systems must share n.  dipole_out as g12_batch_propagate. */
+int g12_batch_propagate_features(g12_batch *b, int64_t nsteps, int32_t every, float *feat_dev, double *dipole_out,
+                                 int64_t *steps_done);
+
 #ifdef __cplusplus
 }
 #endif

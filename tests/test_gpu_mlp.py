@@ -1,0 +1,135 @@
+"""Learned extrapolator kernels on the GPU against the numpy oracle
+(oracle/mlp_oracle.py): forward pass, loss, every parameter gradient, window
+assembly, rollout and feature recording.  Bars: relative Frobenius error
+1e-3 per tensor (the oracle rounds operands to bf16 like the GPU and
+accumulates in FP64; the GPU accumulates in FP32)."""
+import numpy as np
+import pytest
+
+import oracle.mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-3
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    return torch
+
+
+@pytest.fixture(scope="module")
+def learned(g12):
+    from g12kba_b200 import learned
+    return learned
+
+
+def _relf(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("batch", [128, 256])
+def test_loss_and_gradients_vs_oracle(torch, learned, batch):
+    dims = (256, 128, 256, 128, 384)
+    rng = np.random.default_rng(batch)
+    with learned.MLP(dims, max_batch=256, seed=7) as net:
+        params = net.get_params()
+        X = rng.standard_normal((batch, dims[0])).astype(np.float32)
+        Y = rng.standard_normal((batch, dims[4])).astype(np.float32)
+        Xd, Yd = torch.from_numpy(X).cuda(), torch.from_numpy(Y).cuda()
+        out = net.forward(Xd).cpu().numpy()
+        loss = net.loss_grad(Xd, Yd)
+        grads = net.grads()
+    layers = mo.unpack(params, dims)
+    _, As = mo.forward(layers, X)
+    assert _relf(out, As[-1]) <= GRAD_TOL
+    loss_ref, g_ref = mo.loss_grad(layers, X, Y)
+    assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref)
+    g_gpu = mo.unpack(grads, dims)
+    for l in range(4):
+        assert _relf(g_gpu[l][0], g_ref[l][0]) <= GRAD_TOL, ("dW", l, _relf(g_gpu[l][0], g_ref[l][0]))
+        assert _relf(g_gpu[l][1], g_ref[l][1]) <= GRAD_TOL, ("db", l, _relf(g_gpu[l][1], g_ref[l][1]))
+
+
+def test_adam_step_vs_numpy(torch, learned):
+    dims = (128, 128, 128, 128, 128)
+    rng = np.random.default_rng(3)
+    with learned.MLP(dims, max_batch=128, seed=1) as net:
+        p0 = net.get_params()
+        X = torch.from_numpy(rng.standard_normal((128, 128)).astype(np.float32)).cuda()
+        Y = torch.from_numpy(rng.standard_normal((128, 128)).astype(np.float32)).cuda()
+        net.loss_grad(X, Y)
+        g = net.grads()
+        net.adam(1e-2, weight_decay=0.0)
+        p1 = net.get_params()
+    m = 0.1 * g
+    v = 0.001 * g * g
+    ref = p0 - 1e-2 * (m / 0.1) / (np.sqrt(v / 0.001) + 1e-8)
+    assert np.allclose(p1, ref, rtol=1e-5, atol=1e-6)
+
+
+def test_training_fits_a_linear_map(torch, learned):
+    """A learnable task: Y = X A (fixed random A); loss must fall 5x in 300 steps."""
+    dims = (256, 256, 256, 256, 128)
+    rng = np.random.default_rng(4)
+    A = rng.standard_normal((256, 128)) / 16
+    with learned.MLP(dims, max_batch=256, seed=2) as net:
+        losses = []
+        for it in range(300):
+            X = rng.standard_normal((256, 256)).astype(np.float32)
+            Y = (X @ A).astype(np.float32)
+            losses.append(net.loss_grad(torch.from_numpy(X).cuda(), torch.from_numpy(Y).cuda()))
+            net.adam(1e-3)
+    assert np.mean(losses[-20:]) < np.mean(losses[:5]) / 5
+
+
+def test_windows_and_rollout_vs_oracle(torch, learned):
+    n, K, M = 15, 8, 8  # F = 240: K F = M F = 1920 = 15 * 128
+    F = n * (n + 1)
+    dims = (K * F, 128, 128, 128, M * F)
+    rng = np.random.default_rng(5)
+    feat = (0.3 * rng.standard_normal((3, 60, F))).astype(np.float32)
+    mean = feat.mean(axis=(0, 1))
+    with learned.MLP(dims, max_batch=128, seed=3) as net:
+        net.set_norm(K, M, F, mean, 0.5, 0.7, 0.2)
+        fd = torch.from_numpy(feat).cuda()
+        idx = np.array([[0, 7], [2, 30], [1, 51]])
+        X, Y = net.windows(fd, idx)
+        Xr, Yr = mo.windows(feat.astype(np.float64), idx, K, M, mean, 0.5, 0.7, 0.2)
+        assert np.allclose(X.cpu().numpy(), Xr, rtol=1e-6, atol=1e-6)
+        assert np.allclose(Y.cpu().numpy(), Yr, rtol=1e-6, atol=1e-6)
+        params = net.get_params()
+        # rollout of two blocks from t0 = 9 (snaps = 9 + 1 + 2*M = 26)
+        roll = fd[:, :26].clone()
+        roll[:, 10:] = 0
+        net.rollout(roll, 9)
+        roll = roll.cpu().numpy()
+    layers = mo.unpack(params, dims)
+    ref = feat[:, :26].astype(np.float64).copy()
+    ref[:, 10:] = 0
+    t = 9
+    for _ in range(2):
+        Xw, _ = mo.windows(ref, [(i, t) for i in range(3)], K, M, mean, 0.5, 0.7, 0.2)
+        _, As = mo.forward(layers, Xw)
+        for i in range(3):
+            ref[i, t + 1:t + 1 + M] = ref[i, t] + 0.2 * As[-1][i].reshape(M, F)
+        t += M
+    assert np.allclose(roll[:, :10], feat[:, :10])
+    assert _relf(roll[:, 10:], ref[:, 10:]) <= GRAD_TOL
+
+
+def test_batch_features_match_context_trajectory(g12, torch, learned):
+    ps = learned.window_params(3, seed=11, time_steps=40)
+    feat, dip, _ = learned.generate(ps, 40, stride=4)
+    feat = feat.cpu().numpy()
+    for i, p in enumerate(ps):
+        with g12.Context(p) as ctx:
+            ctx.set_state(g12.make_G0(p))
+            ctx.adiabatic_switch()
+            traj, rc = ctx.propagate(40)
+            st = ctx.get_state()
+        # snapshot j = state after step 4(j+1); traj[s] = state at the start of step s
+        want = learned.features(np.concatenate([traj[4::4], st[0][None]], axis=0))
+        assert np.allclose(feat[i], want[: feat.shape[1]], rtol=0, atol=1e-6)
+        assert np.allclose(dip[i], g12.dipole(traj), atol=1e-12)
