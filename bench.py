@@ -217,6 +217,69 @@ def ensemble_measure(g12, local, steps=20, warmup=3, sample=16):
                     f"{len(ps)}/{sample}; from G0 with G2 = 0 (step cost does not depend on the state)"}
 
 
+def learned_measure(g12, local, ntrain=64, ntest=8, T=3000, P=400, train_steps=8000, judge_every=200):
+    """Learned extrapolator on its n=16 family (Ns=8, Nb=2, U ~ U[1,3],
+    quench ~ U[0.5,3] switched on at t=1): trajectories from the batch engine,
+    training on the GPU, rollout of held-out systems from an RK4 prefix of P
+    steps, judged against their RK4 trajectories every `judge_every` steps."""
+    import torch
+    from g12kba_b200 import learned as L
+    ps = L.window_params(ntrain + ntest, seed=5, time_steps=T)
+    t0 = time.perf_counter()
+    feat, _, gen_ms = L.generate(ps, T, stride=1, device=local)
+    ok = L.stable(feat)
+    okn = ok.cpu().numpy()
+    ftr = feat[:ntrain][ok[:ntrain]].contiguous()
+    fte = feat[ntrain:][ok[ntrain:]].contiguous()
+    test_ps = [p for p, k in zip(ps[ntrain:], okn[ntrain:]) if k]
+    del feat
+    ex = L.Extrapolator(16, K=32, M=16, max_batch=512, seed=1)
+    t1 = time.perf_counter()
+    hist = ex.train(ftr, train_steps, batch=512, lr=1e-3, t_min=300)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t1
+    pred, net_ms = ex.rollout(fte[:, :P], T)
+    Tr = pred.shape[1]
+    truth = fte[:, :Tr].cpu().numpy()
+    pred = pred.cpu().numpy()
+    errs = L.running_errors(pred, truth, 16, P - 1)
+    h3, h2 = L.horizon(errs, 1e-3), L.horizon(errs, 1e-2)
+    cks, ce = L.checkpoint_errors(pred, truth, 16, P - 1, judge_every)
+    # plain RK4 on one of these systems (FP64 and the mixed engine)
+    rk = {}
+    for prec in ("fp64", "bf16oz"):
+        with g12.Context(test_ps[0], prec, local) as ctx:
+            ctx.set_state(g12.make_G0(test_ps[0]))
+            ctx.propagate_dipole(20)
+            ctx.propagate_dipole(400)
+            rk[prec] = 400 / (ctx.last_device_ms / 1e3)
+    net_per_traj = (Tr - P) / (net_ms / 1e3)  # snapshots per second per trajectory (all rolled out together)
+    dt = 0.01
+
+    def covered(h):
+        # simulated time per second of "RK4 prefix + network within the horizon"
+        return dt * (P + h) / (P / rk["fp64"] + h / net_per_traj)
+
+    return {
+        "family": "Ns=8 Nb=2 (n=16), t2=0.5, EHM U/(1+r), U~U[1,3], full quench ~U[0.5,3] on Nq=3 at t=1, dt=0.01",
+        "train": {"trajectories": int(ftr.shape[0]), "steps_each": T, "windows_K_M": [32, 16],
+                  "adam_steps": train_steps, "batch": 512, "seconds": train_s, "loss_first": float(hist[:20].mean()),
+                  "loss_last": float(hist[-200:].mean()), "data_device_s": gen_ms / 1e3},
+        "test_trajectories": int(fte.shape[0]), "rk4_prefix_steps": P,
+        "network_rollout": {"snapshots_per_s_per_trajectory": net_per_traj,
+                            "simulated_time_per_s_per_trajectory": dt * net_per_traj,
+                            "device_ms": net_ms, "trajectories": int(fte.shape[0])},
+        "plain_rk4_simulated_time_per_s": {k: dt * v for k, v in rk.items()},
+        "horizon_steps_median_err_le_1e-3": h3, "horizon_steps_median_err_le_1e-2": h2,
+        "judge_every_steps": judge_every,
+        "judge_checkpoint_median_err": {int(c): float(np.median(ce[:, i])) for i, c in enumerate(cks[:10])},
+        "simulated_time_per_s_within_1e-3": covered(h3),
+        "speedup_vs_plain_fp64_within_1e-3": covered(h3) / (dt * rk["fp64"]),
+        "speedup_vs_plain_fp64_within_1e-2": covered(h2) / (dt * rk["fp64"]),
+        "wall_s": time.perf_counter() - t0,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -226,6 +289,7 @@ def main():
     ap.add_argument("--precision", default="bf16oz", choices=["fp64", "tf32x3", "bf16oz", "tf32x6", "fp32"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--skip-as", action="store_true",
                     help="start the timed steps from G0 (profiling runs); the cost of a step does not depend on the state")
     args = ap.parse_args()
@@ -333,6 +397,10 @@ def main():
     if rank == 0 and not args.no_ensemble:
         ensemble = ensemble_measure(g12, local)
 
+    learned = None
+    if rank == 0 and not args.no_learned:
+        learned = learned_measure(g12, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res = reference_cpu(8, 0, max_seconds=20.0)
@@ -354,7 +422,7 @@ def main():
             "speedup_vs_plain_fp64": value / value_fp,
             "g1_max_rel_err_vs_fp64": g1_err,
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline,
-            "kernels": kernels, "ensemble": ensemble, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "kernels": kernels, "ensemble": ensemble, "learned": learned, "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line))
     if pg is not None:

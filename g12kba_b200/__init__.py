@@ -140,6 +140,8 @@ def lib():
         L.g12_mlp_windows.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, _vp, _vp]
         L.g12_mlp_train_windows.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, C.c_float, C.c_float,
                                             _dp]
+        L.g12_mlp_train_pushforward.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, C.c_int32,
+                                                C.c_float, C.c_float, C.c_float, _dp]
         L.g12_mlp_rollout.argtypes = [_vp, _vp, C.c_int32, C.c_int64, C.c_int64, _fp]
         _lib = L
     return _lib

@@ -286,8 +286,27 @@ struct Norm {
 
 // windows -> network input/target.  feat: [traj][snap][F]; idx[b] = (traj, t)
 // with t the last snapshot of the window.  Y may be null (inference).
+__device__ __forceinline__ uint32_t hash32(uint64_t x)
+{
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return uint32_t(x);
+}
+
+// standard normal deviate from a counter (Box-Muller on two hashed uniforms)
+__device__ __forceinline__ float gauss(uint64_t seed, uint64_t ctr)
+{
+    const float u1 = (hash32(seed ^ (2 * ctr)) + 1.0f) * 2.3283064e-10f;   // (0, 1]
+    const float u2 = hash32(seed ^ (2 * ctr + 1)) * 2.3283064e-10f;
+    return sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2);
+}
+
+// noise > 0 adds noise * N(0, 1) to every input (training only)
 __global__ void k_windows(const float *feat, long long snaps, const long long *idx, int batch, Norm nm, float *X,
-                          float *Y)
+                          float *Y, float noise = 0.f, unsigned long long seed = 0)
 {
     const int b = blockIdx.y;
     if (b >= batch) return;
@@ -300,6 +319,7 @@ __global__ void k_windows(const float *feat, long long snaps, const long long *i
         float v;
         if (k == nm.K - 1) v = (xt[f] - nm.mean[f]) / nm.s_abs;
         else v = (base[(t - nm.K + 1 + k) * nm.F + f] - xt[f]) / nm.s_in;
+        if (noise > 0.f) v += noise * gauss(seed, (uint64_t)b * D0 + i);
         X[b * D0 + i] = v;
     }
     if (!Y) return;
@@ -322,6 +342,27 @@ __global__ void k_emit(const float *Yh, long long snaps, const long long *idx, i
     for (long long i = blockIdx.x * blockDim.x + threadIdx.x; i < D4; i += (long long)gridDim.x * blockDim.x) {
         const int m = int(i / nm.F), f = int(i % nm.F);
         base[(t + 1 + m) * nm.F + f] = xt[f] + nm.s_out * Yh[b * D4 + i];
+    }
+}
+
+// scratch[b][j] = feat[traj_b][t_b + j], j < L  (idx = (traj, t) pairs)
+__global__ void k_gather_seq(const float *feat, long long snaps, const long long *idx, int batch, int L, int F,
+                             float *scratch)
+{
+    const int b = blockIdx.y;
+    if (b >= batch) return;
+    const float *src = feat + (idx[2 * b] * snaps + idx[2 * b + 1]) * F;
+    float *dst = scratch + (long long)b * L * F;
+    for (long long i = blockIdx.x * blockDim.x + threadIdx.x; i < (long long)L * F; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+__global__ void k_seq_idx(long long *idx, int batch, long long t)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < batch) {
+        idx[2 * b] = b;
+        idx[2 * b + 1] = t;
     }
 }
 
@@ -352,6 +393,10 @@ struct g12_mlp {
     Norm norm{};
     bool has_norm = false;
     long long adam_t = 0;
+    float *scratch = nullptr;
+    long long scratch_floats = 0;
+    long long *idx2_d = nullptr;
+    unsigned long long noise_ctr = 0;
     std::vector<void *> allocs;
 };
 
@@ -524,7 +569,8 @@ extern "C" int g12_mlp_create(const int32_t *dims, int32_t max_batch, uint64_t s
     }
     if (!malloc_zero(m, &m->dY, size_t(max_batch) * dims[4]) || !malloc_zero(m, &m->Xbuf, size_t(max_batch) * dims[0]) ||
         !malloc_zero(m, &m->Ybuf, size_t(max_batch) * dims[4]) || !malloc_zero(m, &m->loss_d, 1) ||
-        !malloc_zero(m, &m->err_d, 1) || !malloc_zero(m, &m->idx_d, size_t(2) * max_batch))
+        !malloc_zero(m, &m->err_d, 1) || !malloc_zero(m, &m->idx_d, size_t(2) * max_batch) ||
+        !malloc_zero(m, &m->idx2_d, size_t(2) * max_batch))
         return fail(G12_ERR_NOMEM, "out of device memory (MLP)");
     cudaFuncSetAttribute(k_mlp_gemm<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
     cudaFuncSetAttribute(k_mlp_gemm<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem);
@@ -543,6 +589,7 @@ extern "C" int g12_mlp_destroy(g12_mlp *m)
     cudaSetDevice(m->device);
     if (m->s) cudaStreamSynchronize(m->s);
     for (void *p : m->allocs) cudaFree(p);
+    if (m->scratch) cudaFree(m->scratch);
     if (m->s) cudaStreamDestroy(m->s);
     delete m;
     return G12_OK;
@@ -749,4 +796,58 @@ extern "C" int g12_mlp_rollout(g12_mlp *m, float *feat_dev, int32_t ntraj, int64
     if (rc) return rc;
     MCK(cudaGetLastError());
     return check_err(m);
+}
+
+// One optimisation step after `r` blocks of the network's own rollout
+// ("pushforward" training): windows start at (traj, t) of feat_dev, the network
+// predicts r blocks of M snapshots from them (no gradient through those), and
+// the step trains the prediction of the next M true snapshots from the window
+// that now ends in predicted snapshots.  noise > 0 adds Gaussian noise of that
+// size (in normalised units) to every network input of the step.
+extern "C" int g12_mlp_train_pushforward(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t snaps,
+                                         const int64_t *idx, int32_t batch, int32_t r, float noise, float lr,
+                                         float weight_decay, double *loss)
+{
+    if (!m || !m->has_norm || !feat_dev || !idx || r < 0 || batch < 128 || batch % 128 || batch > m->max_batch)
+        return G12_ERR_INVALID;
+    const Norm &nm = m->norm;
+    const int L = nm.K + (r + 1) * nm.M;
+    for (int b = 0; b < batch; ++b)
+        if (idx[2 * b] < 0 || idx[2 * b] >= ntraj || idx[2 * b + 1] < nm.K - 1 ||
+            idx[2 * b + 1] - (nm.K - 1) + L > snaps) {
+            m->err = "window out of the trajectory";
+            return G12_ERR_INVALID;
+        }
+    MCK(cudaSetDevice(m->device));
+    const long long need = (long long)batch * L * nm.F;
+    if (need > m->scratch_floats) {
+        MCK(cudaStreamSynchronize(m->s));
+        if (m->scratch) cudaFree(m->scratch);
+        m->scratch = nullptr;
+        m->scratch_floats = 0;
+        MCK(cudaMalloc(&m->scratch, sizeof(float) * need));
+        m->scratch_floats = need;
+    }
+    std::vector<long long> first(size_t(2) * batch);
+    for (int b = 0; b < batch; ++b) {
+        first[2 * b] = idx[2 * b];
+        first[2 * b + 1] = idx[2 * b + 1] - (nm.K - 1);
+    }
+    MCK(cudaMemcpyAsync(m->idx_d, first.data(), sizeof(long long) * first.size(), cudaMemcpyHostToDevice, m->s));
+    k_gather_seq<<<dim3(32, batch), 256, 0, m->s>>>(feat_dev, snaps, m->idx_d, batch, L, nm.F, m->scratch);
+    k_seq_idx<<<(batch + 127) / 128, 128, 0, m->s>>>(m->idx2_d, batch, nm.K - 1);
+    MCK(cudaGetLastError());
+    for (int q = 0; q < r; ++q) {
+        k_windows<<<dim3(64, batch), 256, 0, m->s>>>(m->scratch, L, m->idx2_d, batch, nm, m->Xbuf, nullptr);
+        int rc = forward(m, m->Xbuf, batch);
+        if (rc) return rc;
+        k_emit<<<dim3(32, batch), 256, 0, m->s>>>(m->A[3], L, m->idx2_d, batch, nm, m->scratch);
+        k_advance_idx<<<(batch + 127) / 128, 128, 0, m->s>>>(m->idx2_d, batch, nm.M);
+    }
+    k_windows<<<dim3(64, batch), 256, 0, m->s>>>(m->scratch, L, m->idx2_d, batch, nm, m->Xbuf, m->Ybuf, noise,
+                                                 0x9E3779B97F4A7C15ULL + m->noise_ctr++);
+    MCK(cudaGetLastError());
+    int rc = g12_mlp_loss_grad(m, m->Xbuf, m->Ybuf, batch, loss);
+    if (rc) return rc;
+    return g12_mlp_adam(m, lr, 0.9f, 0.999f, 1e-8f, weight_decay);
 }

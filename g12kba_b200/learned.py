@@ -198,6 +198,14 @@ class MLP:
                                               weight_decay, C.byref(loss)))
         return loss.value
 
+    def train_pushforward(self, feat, idx, r, lr, noise=0.0, weight_decay=0.0):
+        idx = np.ascontiguousarray(idx, np.int64)
+        loss = C.c_double()
+        self._chk(lib().g12_mlp_train_pushforward(self.h, C.c_void_p(feat.data_ptr()), feat.shape[0], feat.shape[1],
+                                                  idx.ctypes.data_as(C.POINTER(C.c_int64)), idx.shape[0], r, noise,
+                                                  lr, weight_decay, C.byref(loss)))
+        return loss.value
+
     def rollout(self, feat, t0):
         """Fill snapshots t0+1.. of every trajectory of feat (in place); device ms."""
         _torch().cuda.synchronize()
@@ -231,20 +239,27 @@ class Extrapolator:
         self.norm = (mean.float().cpu().numpy(), max(s_in, 1e-6), max(s_abs, 1e-6), max(s_out, 1e-6))
         self.mlp.set_norm(self.K, self.M, self.F, self.norm[0], self.norm[1], self.norm[2], self.norm[3])
 
-    def train(self, feat, steps, batch=512, lr=1e-3, lr_min=1e-5, weight_decay=0.0, t_min=0, seed=0, log=None):
-        """Adam on random windows (cosine learning-rate decay); returns the loss
-        history (one value per step)."""
+    def train(self, feat, steps, batch=512, lr=1e-3, lr_min=1e-5, weight_decay=0.0, t_min=0, seed=0, log=None,
+              pushforward=0, noise=0.0, warm=0.25):
+        """Adam on random windows (cosine learning-rate decay); after the first
+        `warm` fraction of the steps, each step first rolls the network forward
+        r ~ U{0..pushforward} blocks and trains on the windows it produced.
+        Returns the loss history (one value per step)."""
         if self.norm is None:
             self.fit_norm(feat, t_min)
         rng = np.random.default_rng(seed)
         ntraj, snaps = feat.shape[0], feat.shape[1]
         lo = max(self.K - 1, t_min)
-        hi = snaps - self.M  # t + M < snaps
         hist = []
         for it in range(steps):
-            idx = np.stack([rng.integers(0, ntraj, batch), rng.integers(lo, hi, batch)], axis=1)
             a = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * it / max(1, steps)))
-            hist.append(self.mlp.train_windows(feat, idx, a, weight_decay))
+            r = int(rng.integers(0, pushforward + 1)) if (pushforward and it >= warm * steps) else 0
+            hi = snaps - (r + 1) * self.M  # the window plus r + 1 blocks fit
+            idx = np.stack([rng.integers(0, ntraj, batch), rng.integers(lo, hi, batch)], axis=1)
+            if r == 0 and noise == 0.0:
+                hist.append(self.mlp.train_windows(feat, idx, a, weight_decay))
+            else:
+                hist.append(self.mlp.train_pushforward(feat, idx, r, a, noise, weight_decay))
             if log and (it % max(1, steps // 20) == 0 or it == steps - 1):
                 log(f"step {it} lr {a:.2e} loss {hist[-1]:.3e}")
         return np.array(hist)
@@ -264,3 +279,40 @@ class Extrapolator:
 def dipole_error(p, p_ref):
     """max_t |p - p_ref| / max(max_t |p_ref|, 1e-12) (the metric's definition)."""
     return float(np.max(np.abs(p - p_ref)) / max(np.max(np.abs(p_ref)), 1e-12))
+
+
+def naive_rollout(prefix, total):
+    """The method without a network past the exact prefix: hold the last
+    snapshot (the comparator the tests measure the network's gain against)."""
+    torch = _torch()
+    out = torch.empty((prefix.shape[0], total, prefix.shape[2]), dtype=prefix.dtype, device=prefix.device)
+    out[:, : prefix.shape[1]] = prefix
+    out[:, prefix.shape[1]:] = prefix[:, -1:]
+    return out
+
+
+def checkpoint_errors(pred, truth, n, t0, every):
+    """Dipole error of a rollout against the RK4 trajectory at the judge's
+    checkpoints: for each checkpoint c (every `every` snapshots after t0),
+    max over snapshots t0 < s <= c of |p - p_ref| / max|p_ref| (per trajectory).
+    Returns (checkpoints, errors [ntraj][ncheck])."""
+    pr = dipole_from_features(np.asarray(pred), n)
+    pt = dipole_from_features(np.asarray(truth), n)
+    amp = np.maximum(np.max(np.abs(pt), axis=1), 1e-12)
+    e = np.maximum.accumulate(np.abs(pr[:, t0 + 1:] - pt[:, t0 + 1:]) / amp[:, None], axis=1)
+    cks = np.arange(every, e.shape[1] + 1, every)
+    return t0 + cks, e[:, cks - 1]
+
+
+def horizon(errors_cum, tol):
+    """Snapshots after the prefix for which the median running error stays <= tol."""
+    med = np.median(errors_cum, axis=0)
+    bad = np.nonzero(med > tol)[0]
+    return int(bad[0]) if bad.size else int(med.size)
+
+
+def running_errors(pred, truth, n, t0):
+    pr = dipole_from_features(np.asarray(pred), n)
+    pt = dipole_from_features(np.asarray(truth), n)
+    amp = np.maximum(np.max(np.abs(pt), axis=1), 1e-12)
+    return np.maximum.accumulate(np.abs(pr[:, t0 + 1:] - pt[:, t0 + 1:]) / amp[:, None], axis=1)

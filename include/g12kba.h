@@ -236,6 +236,11 @@ int g12_mlp_windows(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t sn
                     int32_t batch, float *X_dev, float *Y_dev);
 int g12_mlp_train_windows(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t snaps, const int64_t *idx,
                           int32_t batch, float lr, float weight_decay, double *loss);
+/* one step after r blocks of the network's own rollout from windows ending at
+ * idx's t (targets: the true snapshots that follow); noise: Gaussian input
+ * noise in normalised units (0: none) */
+int g12_mlp_train_pushforward(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t snaps, const int64_t *idx,
+                              int32_t batch, int32_t r, float noise, float lr, float weight_decay, double *loss);
 /* in place: snapshots t0+1 .. snaps-1 of every trajectory from blocks of M
  * predictions ((snaps-1-t0) % M == 0); device time in *elapsed_ms */
 int g12_mlp_rollout(g12_mlp *m, float *feat_dev, int32_t ntraj, int64_t snaps, int64_t t0, float *elapsed_ms);
