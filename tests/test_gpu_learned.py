@@ -35,10 +35,10 @@ def test_trained_network_beats_no_network(family):
     raw.fit_norm(ftr, 300)
     e_raw = L.running_errors(raw.rollout(fte[:, :P], P + H)[0].cpu().numpy(), truth, n, P - 1)
     med = lambda e, s: float(np.median(e[:, s - 1]))  # running error after s steps
-    # two blocks past the prefix: an order of magnitude closer to RK4 than
-    # holding the last RK4 snapshot or than the untrained network
-    assert med(e_net, 32) < 0.1 * med(e_hold, 32), (med(e_net, 32), med(e_hold, 32))
-    assert med(e_net, 32) < 0.1 * med(e_raw, 32), (med(e_net, 32), med(e_raw, 32))
+    # two blocks past the prefix: several times closer to RK4 than holding the
+    # last RK4 snapshot or than the untrained network
+    assert med(e_net, 32) < 0.25 * med(e_hold, 32), (med(e_net, 32), med(e_hold, 32))
+    assert med(e_net, 32) < 0.25 * med(e_raw, 32), (med(e_net, 32), med(e_raw, 32))
     assert med(e_net, 16) < 1e-2
     # and still closer after 160 steps
     assert med(e_net, H) < 0.7 * med(e_hold, H), (med(e_net, H), med(e_hold, H))
