@@ -408,6 +408,7 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
         if (rc) return fail(rc);
         d.Qt = ctx->mixed.s.Qt;  // k_prep writes the transposed tables the epilogue reads
         d.Rtt = ctx->mixed.s.Rtt;
+        d.ozb = ctx->mixed.ozb;  // k_prep also writes the digits of h for the tcgen05 GEMM
     }
     if (ensure_sched(ctx, 1024)) return fail(G12_ERR_CUDA);
     *out = ctx;

@@ -31,6 +31,7 @@
 //   matrices X, with (L, R) = (h, h^T) or (h^T, h).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -48,6 +49,7 @@ struct Dev {
     double2 *Y1, *G1t0, *G1t1, *RK1, *h, *Ix, *comm_dbg, *K1_dbg;
     double2 *Y2, *RK2, *TMP0, *TMP1, *TAB, *D, *Q, *Rt;
     double2 *Qt, *Rtt;  // transposed table copies (symmetric engine), or null
+    unsigned char *ozb; // bf16 digit tiles of h for the tcgen05 digit GEMM (symmetric engine), or null
     double2 *traj;
     double *dip;
     long long traj_cap;
@@ -195,6 +197,47 @@ __host__ __device__ inline int prep_pair_blocks(long long n2) { return int((n2 +
 inline int prep_blocks(long long n2) { return prep_pair_blocks(n2) + int((n2 + kPrepWarps * 32 - 1) / (kPrepWarps * 32)); }
 inline size_t prep_smem() { return size_t(kPrepWarps) * 4 * kMaxN * sizeof(double2); }
 
+// Exact bf16 digits of the real form of h^T for the tcgen05 digit GEMM of the
+// symmetric engine (sym_oz.cuh), written once per stage by the threads that
+// compute h (n = 16 or 32: each 128-thread block holds whole rows of h).
+// B row j = po*n + mu1, column kk = pi*n + rho:
+//   (po, pi) = (0, 0): Re h, (0, 1): -Im h, (1, 0): Im h, (1, 1): Re h  at h[mu1][rho];
+// each row is scaled by 2^(20 - e), e = exponent of its largest |entry|, and
+// split by successive round-to-nearest into 4 digits (|d0| <= 128, |d1..d3| <= 64).
+// Layout: 4 tiles of 2n rows x 128 bytes (128-byte swizzle, K-major), then
+// the 2n row scales 2^(e - 6) as floats.
+__device__ __forceinline__ void h_digits(const Dev &d, double2 hv, int x)
+{
+    const int n = d.n;
+    const int mu1 = x / n, rho = x % n;
+    double m = fmax(fabs(hv.x), fabs(hv.y));
+    for (int o = n / 2; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    const int e = (m > 0.0) ? ilogb(m) : 0;
+    const int tile = 2 * n * 128;
+    const double vals[4] = {hv.x, -hv.y, hv.y, hv.x};
+#pragma unroll
+    for (int idx = 0; idx < 4; ++idx) {
+        const int j = (idx >> 1) * n + mu1, kk = (idx & 1) * n + rho;
+        double r = ldexp(vals[idx], 20 - e);
+        double dg[4];
+        dg[0] = rint(r / 16384.0);
+        r -= dg[0] * 16384.0;
+        dg[1] = rint(r / 128.0);
+        r -= dg[1] * 128.0;
+        dg[2] = rint(r);
+        r -= dg[2];
+        dg[3] = rint(r * 128.0);
+        const int byte = j * 128 + ((((kk >> 3) ^ (j & 7)) << 4) | ((kk & 7) << 1));
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            *reinterpret_cast<__nv_bfloat16 *>(d.ozb + q * tile + byte) = __float2bfloat16_rn(float(dg[q]));
+    }
+    if (rho == 0) {
+        float *sc = reinterpret_cast<float *>(d.ozb + 4 * tile);
+        sc[mu1] = sc[n + mu1] = float(ldexp(1.0, e - 6));
+    }
+}
+
 __device__ __forceinline__ void prep_body(const Dev &d, int k, int bx)
 {
     if (!*d.active) return;
@@ -205,7 +248,12 @@ __device__ __forceinline__ void prep_body(const Dev &d, int k, int bx)
     const int pair_blocks = prep_pair_blocks(n2);
     if (bx >= pair_blocks) {
         const long long x = (long long)(bx - pair_blocks) * blockDim.x + threadIdx.x;
-        if (x < n2) d.h[x] = h_entry(d, G, int(x / n), int(x % n), st);
+        double2 hv = make_double2(0.0, 0.0);
+        if (x < n2) {
+            hv = h_entry(d, G, int(x / n), int(x % n), st);
+            d.h[x] = hv;
+        }
+        if (d.ozb) h_digits(d, hv, int(x));
         return;
     }
     extern __shared__ double2 sm[];

@@ -24,6 +24,7 @@
 #include "g12kba.h"
 #include "internal.h"
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 

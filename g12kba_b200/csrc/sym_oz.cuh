@@ -326,3 +326,280 @@ __global__ void __launch_bounds__(kOzThreads, 2) k_sym_gemm_oz(SymDev s, int k)
 }
 
 }  // namespace g12
+
+namespace g12 {
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void named_sync(int id, int nthreads)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// Warp-specialised, persistent version of k_sym_gemm_oz (same tiles, digits
+// and products).  Roles (10 warps):
+//   warp 0      TMA producer: FP32 A tiles into a 2-stage ring
+//   warp 1      one thread issues the 10 digit products per tile into one of
+//               two TMEM accumulator sets
+//   warps 2-5   digit split, one thread per A row (row max, exponent, 4 bf16
+//               digit rows)
+//   warps 6-9   epilogue: TMEM -> FP32 combination -> staging -> W = T1 + e(T1)
+// so the loads of tile i+2, the digits of tile i+1, the products of tile i+1
+// and the epilogue of tile i overlap.  Every wait is bounded.
+constexpr int kOz2Threads = 320;
+
+template <int NN>
+struct Oz2Shape {
+    static constexpr int N = 2 * NN;            // UMMA N
+    static constexpr int KF = 2 * NN;           // FP32 values per A row
+    static constexpr int KB = KF / 32;          // 128-byte TMA boxes per A row
+    static constexpr int DC = KF / 8;           // 16-byte digit chunks per row (of 8 in a 128-byte row)
+    static constexpr int KS = KF / 16;          // 32-byte K steps per product
+    static constexpr int CPT = 128 / NN;
+    static constexpr int A_STAGE = KB * 128 * 128;   // one FP32 tile
+    static constexpr int D_BYTES = 128 * 128;        // one digit tile (128 rows x 128 B)
+    static constexpr int B_BYTES = N * 128;
+    static constexpr int ACC = kOzLevels * N;        // TMEM columns per accumulator set
+    static constexpr int TMEM_COLS = 2 * ACC;        // 512 (n = 32) or 256 (n = 16)
+    static constexpr int S_LD = N + 1;
+    static constexpr int OFF_A = 0;                                  // 2 stages
+    static constexpr int OFF_D = OFF_A + 2 * A_STAGE;                // kOzDigits digit tiles
+    static constexpr int OFF_B = OFF_D + kOzDigits * D_BYTES;        // kOzDigits B digit tiles
+    static constexpr int OFF_S = OFF_B + kOzDigits * B_BYTES;        // 128 x S_LD floats
+    static constexpr int OFF_E = OFF_S + 128 * S_LD * 4;             // eA[3][128], eB[N], sB[N]
+    static constexpr int OFF_BAR = OFF_E + (3 * 128 + N) * 4 + N * 4;
+    static constexpr int SMEM = OFF_BAR + 16 * 8 + 1024;
+    static_assert(SMEM <= 227 * 1024, "shared memory");
+};
+
+template <int NN>
+__global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k, const __grid_constant__ CUtensorMap tmap)
+{
+    using Sh = Oz2Shape<NN>;
+    if (!*s.d.active) return;
+    extern __shared__ unsigned char smraw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
+    unsigned char *As = sm + Sh::OFF_A;
+    unsigned char *Ds = sm + Sh::OFF_D;
+    unsigned char *Bd = sm + Sh::OFF_B;
+    float *S = reinterpret_cast<float *>(sm + Sh::OFF_S);
+    int *eA = reinterpret_cast<int *>(sm + Sh::OFF_E);      // [3][128]
+    float *sB = reinterpret_cast<float *>(eA + 3 * 128 + Sh::N);  // [N]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Sh::OFF_BAR);
+    uint64_t *full_a = bar, *empty_a = bar + 2, *dig_full = bar + 4, *dig_empty = bar + 5, *acc_full = bar + 6,
+             *acc_empty = bar + 8;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 10);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long n2 = (long long)NN * NN;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(Sh::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        mbar_init(&full_a[0], 1);
+        mbar_init(&full_a[1], 1);
+        mbar_init(&empty_a[0], 128);
+        mbar_init(&empty_a[1], 128);
+        mbar_init(dig_full, 128);
+        mbar_init(dig_empty, 1);
+        mbar_init(&acc_full[0], 1);
+        mbar_init(&acc_full[1], 1);
+        mbar_init(&acc_empty[0], 128);
+        mbar_init(&acc_empty[1], 128);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // digit tiles start at zero (the n = 16 rows fill half of each 128-byte row);
+    // the B digit tiles and row scales of h were written by k_prep (h_digits)
+    for (int i = tid; i < kOzDigits * Sh::D_BYTES / 16; i += blockDim.x)
+        reinterpret_cast<uint4 *>(Ds)[i] = make_uint4(0, 0, 0, 0);
+    const uint4 *bsrc = reinterpret_cast<const uint4 *>(s.d.ozb);
+    for (int i = tid; i < kOzDigits * Sh::B_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4 *>(Bd)[i] = bsrc[i];
+    const float *sbsrc = reinterpret_cast<const float *>(s.d.ozb + kOzDigits * Sh::B_BYTES);
+    for (int j = tid; j < Sh::N; j += blockDim.x) sB[j] = sbsrc[j];
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int ntiles = 2 * s.gemm_tiles;
+    const int my_tiles = (ntiles - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x);
+    bool ok = true;
+
+    if (warp == 0) {
+        // ---- TMA producer
+        if (lane == 0) {
+            int issued = 0;
+            for (int i = 0; i < my_tiles && ok; ++i) {
+                const int tile = blockIdx.x + i * gridDim.x;
+                const int t = tile / s.gemm_tiles, g = tile % s.gemm_tiles, sa = i & 1;
+                if (i >= 2 && !mbar_wait(&empty_a[sa], ((i - 2) >> 1) & 1)) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&full_a[sa], Sh::A_STAGE);
+                for (int slot = 0; slot < Sh::CPT; ++slot) {
+                    const int c = s.gemm_c[g * Sh::CPT + slot];
+                    for (int kb = 0; kb < Sh::KB; ++kb)
+                        tma_load_4d(As + sa * Sh::A_STAGE + kb * 128 * 128 + slot * NN * 128, &tmap, &full_a[sa],
+                                    kb * 32, c, 0, t);
+                }
+                issued = i + 1;
+            }
+            if (!ok) {
+                atomicExch(s.err, 4);
+                // let the copies in flight land before the CTA exits
+                for (int i = (issued >= 2 ? issued - 2 : 0); i < issued; ++i) mbar_wait(&full_a[i & 1], (i >> 1) & 1);
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = umma_idesc_bf16(Sh::N);
+            const uint32_t ab = smem_u32(Ds), bb = smem_u32(Bd);
+            int done = 0;
+            for (int i = 0; i < my_tiles; ++i) {
+                const int b = i & 1;
+                if (!mbar_wait(dig_full, i & 1) || (i >= 2 && !mbar_wait(&acc_empty[b], ((i - 2) >> 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t acc0 = tmem + b * Sh::ACC;
+                for (int L = 0; L < kOzLevels; ++L) {
+                    uint32_t acc = 0;
+                    for (int ii = 0; ii <= L; ++ii) {
+                        const int jj = L - ii;
+                        for (int ks = 0; ks < Sh::KS; ++ks) {
+                            umma_bf16(acc0 + L * Sh::N, umma_desc_sw128(ab + ii * Sh::D_BYTES + ks * 32),
+                                      umma_desc_sw128(bb + jj * Sh::B_BYTES + ks * 32), idesc, acc);
+                            acc = 1;
+                        }
+                    }
+                }
+                umma_commit(&acc_full[b]);
+                umma_commit(dig_empty);
+                done = i + 1;
+            }
+            if (!ok) {
+                atomicExch(s.err, 5);
+                if (done > 0) mbar_wait(dig_empty, (done - 1) & 1);  // the last products have landed
+            }
+        }
+    } else if (warp < 6) {
+        // ---- digit split: thread -> row m
+        const int m = tid - 64;
+        const int sw = m & 7;
+        for (int i = 0; i < my_tiles; ++i) {
+            const int sa = i & 1;
+            if (!mbar_wait(&full_a[sa], (i >> 1) & 1) || (i >= 1 && !mbar_wait(dig_empty, (i - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            float v[Sh::KF];
+            const unsigned char *row = As + sa * Sh::A_STAGE + m * 128;
+#pragma unroll
+            for (int kb = 0; kb < Sh::KB; ++kb)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const float4 q = *reinterpret_cast<const float4 *>(row + kb * 128 * 128 + ((j ^ sw) << 4));
+                    v[kb * 32 + 4 * j + 0] = q.x;
+                    v[kb * 32 + 4 * j + 1] = q.y;
+                    v[kb * 32 + 4 * j + 2] = q.z;
+                    v[kb * 32 + 4 * j + 3] = q.w;
+                }
+            mbar_arrive(&empty_a[sa]);
+            float mx = 0.f;
+#pragma unroll
+            for (int x = 0; x < Sh::KF; ++x) mx = fmaxf(mx, fabsf(v[x]));
+            const int e = (mx > 0.f) ? max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, -100) : 0;
+            eA[(i % 3) * 128 + m] = e;
+            const float sc = pow2f(20 - e);
+#pragma unroll
+            for (int ch = 0; ch < Sh::DC; ++ch) {
+                uint32_t w[kOzDigits][4];
+#pragma unroll
+                for (int pr = 0; pr < 4; ++pr) {
+                    float d0[kOzDigits], d1[kOzDigits];
+                    oz_digits(v[ch * 8 + 2 * pr] * sc, d0);
+                    oz_digits(v[ch * 8 + 2 * pr + 1] * sc, d1);
+#pragma unroll
+                    for (int q = 0; q < kOzDigits; ++q) {
+                        const __nv_bfloat162 p2 = __floats2bfloat162_rn(d0[q], d1[q]);
+                        w[q][pr] = *reinterpret_cast<const uint32_t *>(&p2);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kOzDigits; ++q)
+                    *reinterpret_cast<uint4 *>(Ds + q * Sh::D_BYTES + m * 128 + ((ch ^ sw) << 4)) =
+                        make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(dig_full);
+        }
+        if (!ok) atomicExch(s.err, 6);
+    } else {
+        // ---- epilogue: warp quadrant q reads TMEM lanes 32q..32q+31
+        const int quad = warp & 3;
+        const int row = quad * 32 + lane;
+        const int et = tid - 192;  // 0..127
+        for (int i = 0; i < my_tiles; ++i) {
+            const int b = i & 1;
+            const int tile = blockIdx.x + i * gridDim.x;
+            const int t = tile / s.gemm_tiles, g = tile % s.gemm_tiles;
+            if (!mbar_wait(&acc_full[b], (i >> 1) & 1)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const float sa = pow2f(eA[(i % 3) * 128 + row] - 6);
+            const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * Sh::ACC;
+#pragma unroll
+            for (int cb = 0; cb < Sh::N; cb += 32) {
+                float acc[32];
+#pragma unroll
+                for (int x = 0; x < 32; ++x) acc[x] = 0.f;
+#pragma unroll
+                for (int L = kOzLevels - 1; L >= 0; --L) {
+                    float w[32];
+                    tmem_ld32(ta + L * Sh::N + cb, w);
+                    // sum_L 2^(-7L) P_L, smallest level first (FP32, round to nearest)
+#pragma unroll
+                    for (int x = 0; x < 32; ++x) acc[x] = fmaf(acc[x], 0x1p-7f, w[x]);
+                }
+#pragma unroll
+                for (int x = 0; x < 32; ++x) S[row * Sh::S_LD + cb + x] = acc[x] * sa * sB[cb + x];
+            }
+            tc_fence_before();
+            mbar_arrive(&acc_empty[b]);
+            named_sync(1, 128);
+            float *Wg = s.W + t * 2 * s.n4;
+#pragma unroll 1
+            for (int sp = 0; sp < Sh::CPT * 2; ++sp) {
+                const int slot = sp >> 1, part = sp & 1;
+                const int ps = s.gemm_partner[g * Sh::CPT + slot];
+                float *Wrow = Wg + ((long long)s.gemm_c[g * Sh::CPT + slot] * 2 + part) * n2;
+#pragma unroll 4
+                for (int r = et; r < NN * NN; r += 128) {
+                    const int mu1 = r % NN, mu2 = r / NN;
+                    Wrow[r] = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] +
+                              S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
+                }
+            }
+            named_sync(1, 128);
+        }
+        if (!ok) atomicExch(s.err, 7);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Sh::TMEM_COLS) : "memory");
+}
+
+}  // namespace g12
