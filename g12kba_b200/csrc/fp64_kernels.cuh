@@ -198,12 +198,12 @@ inline int prep_blocks(long long n2) { return prep_pair_blocks(n2) + int((n2 + k
 inline size_t prep_smem() { return size_t(kPrepWarps) * 4 * kMaxN * sizeof(double2); }
 
 // Exact bf16 digits of the real form of h^T for the tcgen05 digit GEMM of the
-// symmetric engine (sym_oz.cuh), written once per stage by the threads that
-// compute h (n = 16 or 32: each 128-thread block holds whole rows of h).
+// symmetric engine (sym_oz.cuh, k_sym_gemm_oz2), written once per stage by the
+// threads that compute h (n = 16 or 32: each 128-thread block holds whole rows of h).
 // B row j = po*n + mu1, column kk = pi*n + rho:
 //   (po, pi) = (0, 0): Re h, (0, 1): -Im h, (1, 0): Im h, (1, 1): Re h  at h[mu1][rho];
-// each row is scaled by 2^(20 - e), e = exponent of its largest |entry|, and
-// split by successive round-to-nearest into 4 digits (|d0| <= 128, |d1..d3| <= 64).
+// each row is scaled by 2^(30 - e), e = exponent of its largest |entry|, and
+// split by successive round-to-nearest into 4 digits (|d| <= 128).
 // Layout: 4 tiles of 2n rows x 128 bytes (128-byte swizzle, K-major), then
 // the 2n row scales 2^(e - 6) as floats.
 __device__ __forceinline__ void h_digits(const Dev &d, double2 hv, int x)
@@ -218,15 +218,15 @@ __device__ __forceinline__ void h_digits(const Dev &d, double2 hv, int x)
 #pragma unroll
     for (int idx = 0; idx < 4; ++idx) {
         const int j = (idx >> 1) * n + mu1, kk = (idx & 1) * n + rho;
-        double r = ldexp(vals[idx], 20 - e);
+        double r = ldexp(vals[idx], 30 - e);
         double dg[4];
-        dg[0] = rint(r / 16384.0);
-        r -= dg[0] * 16384.0;
-        dg[1] = rint(r / 128.0);
-        r -= dg[1] * 128.0;
-        dg[2] = rint(r);
-        r -= dg[2];
-        dg[3] = rint(r * 128.0);
+        dg[0] = rint(r * 0x1p-24);
+        r -= dg[0] * 0x1p24;
+        dg[1] = rint(r * 0x1p-16);
+        r -= dg[1] * 0x1p16;
+        dg[2] = rint(r * 0x1p-8);
+        r -= dg[2] * 0x1p8;
+        dg[3] = rint(r);
         const int byte = j * 128 + ((((kk >> 3) ^ (j & 7)) << 4) | ((kk & 7) << 1));
 #pragma unroll
         for (int q = 0; q < 4; ++q)

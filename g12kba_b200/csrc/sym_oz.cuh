@@ -51,17 +51,39 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t
         : "memory");
 }
 
-// digits of x (already scaled so that |x| < 2^21): x = d0 2^14 + d1 2^7 + d2 + d3 2^-7 + r
+// Round to the nearest integer (ties to even) for |x| < 2^22 by adding and
+// removing 1.5 * 2^23: the sum's rounding discards exactly the fraction.  Two
+// full-rate FP32 operations instead of the conversion pipe's rounding.
+__device__ __forceinline__ float rint_small(float x)
+{
+    return __fadd_rn(__fadd_rn(x, 12582912.0f), -12582912.0f);
+}
+
+// rint_small(a * b) with one rounding (the product of a and a power of two b is exact)
+__device__ __forceinline__ float rint_small_mul(float a, float b)
+{
+    return __fadd_rn(__fmaf_rn(a, b, 12582912.0f), -12582912.0f);
+}
+
+// digits of x (already scaled so that |x| < 2^21): x = d0 2^14 + d1 2^7 + d2 + d3 2^-7 + r,
+// every step exact except the final remainder
 __device__ __forceinline__ void oz_digits(float x, float (&d)[kOzDigits])
 {
     float r = x;
-    d[0] = rintf(r * (1.0f / 16384.0f));
-    r -= d[0] * 16384.0f;
-    d[1] = rintf(r * (1.0f / 128.0f));
-    r -= d[1] * 128.0f;
-    d[2] = rintf(r);
-    r -= d[2];
-    d[3] = rintf(r * 128.0f);
+    d[0] = rint_small_mul(r, 1.0f / 16384.0f);
+    r = __fmaf_rn(-d[0], 16384.0f, r);
+    d[1] = rint_small_mul(r, 1.0f / 128.0f);
+    r = __fmaf_rn(-d[1], 128.0f, r);
+    d[2] = rint_small(r);
+    r = __fadd_rn(r, -d[2]);
+    d[3] = rint_small_mul(r, 128.0f);
+}
+
+// two small integers (|d| <= 256, exact in bf16) -> packed bf16x2 (a in the low
+// half): the bf16 of such a value is the upper half of its FP32 bit pattern
+__device__ __forceinline__ uint32_t bf16x2_of_ints(float a, float b)
+{
+    return __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x7632);
 }
 
 __device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }  // |e| < 127
@@ -78,6 +100,55 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// TMEM loads without the completion wait (several loads, then tmem_wait_ld on each)
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, float (&v)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
+          "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15]),
+          "=f"(v[16]), "=f"(v[17]), "=f"(v[18]), "=f"(v[19]), "=f"(v[20]), "=f"(v[21]), "=f"(v[22]), "=f"(v[23]),
+          "=f"(v[24]), "=f"(v[25]), "=f"(v[26]), "=f"(v[27]), "=f"(v[28]), "=f"(v[29]), "=f"(v[30]), "=f"(v[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, float (&v)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
+          "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
+        : "r"(taddr));
+}
+
+// tcgen05.wait::ld that also names the loaded registers, so no use of them
+// can be scheduled before the wait
+__device__ __forceinline__ void tmem_wait_ld(float (&v)[32])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]), "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]), "+f"(v[15]), "+f"(v[16]), "+f"(v[17]), "+f"(v[18]), "+f"(v[19]), "+f"(v[20]), "+f"(v[21]), "+f"(v[22]), "+f"(v[23]), "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]), "+f"(v[28]), "+f"(v[29]), "+f"(v[30]), "+f"(v[31])
+                 :
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_ld(float (&v)[16])
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]), "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]), "+f"(v[15])
+                 :
+                 : "memory");
+}
+
+template <int W>
+__device__ __forceinline__ void tmem_ldw_nowait(uint32_t taddr, float (&v)[W])
+{
+    if constexpr (W == 32) tmem_ld32_nowait(taddr, v);
+    else tmem_ld16_nowait(taddr, v);
 }
 
 template <int W>
@@ -339,17 +410,45 @@ __device__ __forceinline__ void named_sync(int id, int nthreads)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Warp-specialised, persistent version of k_sym_gemm_oz (same tiles, digits
-// and products).  Roles (10 warps):
-//   warp 0      TMA producer: FP32 A tiles into a 2-stage ring
+// Warp-specialised, persistent digit GEMM (same tiles as k_sym_gemm_oz) with
+// four 8-bit digits per operand:
+//   a = 2^(e - 6) (d0 + d1 2^-8 + d2 2^-16 + d3 2^-24),  |d_i| <= 128 (exact in bf16),
+// obtained by successive round-to-nearest of a 2^(30 - e) (e = exponent of the
+// row maximum): every FP32 value within 2^8 of its row maximum is represented
+// exactly, the rest to 2^-32 of the maximum.  (Three digits, with a remainder of
+// 2^-23 of the row maximum, let G1 drift to 4e-6 over 10,000 steps at n = 32.)
+// Products with digit levels i + j = L <= 3 accumulate in TMEM accumulator L:
+// |sum| <= 4 * K * 128 * 128 <= 2^22 < 2^24, exact in FP32 whatever the
+// accumulator's rounding; T1 = 2^(e_m - 6) 2^(e_j - 6) sum_L 2^(-8L) P_L.
+// Roles (18 warps):
+//   warp 0      TMA producer: FP32 A tiles into a 2-stage ring (starts as soon
+//               as the barriers exist)
 //   warp 1      one thread issues the 10 digit products per tile into one of
 //               two TMEM accumulator sets
-//   warps 2-5   digit split, one thread per A row (row max, exponent, 4 bf16
+//   warps 2-9   digit split, two threads per A row (row max, exponent, 4 bf16
 //               digit rows)
-//   warps 6-9   epilogue: TMEM -> FP32 combination -> staging -> W = T1 + e(T1)
-// so the loads of tile i+2, the digits of tile i+1, the products of tile i+1
-// and the epilogue of tile i overlap.  Every wait is bounded.
-constexpr int kOz2Threads = 320;
+//   warps 10-17 epilogue, one per TMEM lane quadrant and part (real or
+//               imaginary half of the columns): TMEM -> FP32 combination ->
+//               staging -> W = T1 + e(T1)
+// so the loads of tile i+2, the digits and products of tile i+1 and the
+// epilogue of tile i overlap.  The digits of h come from k_prep
+// (h_digits).  Every wait is bounded.
+constexpr int kOz2Threads = 576;
+constexpr int kOz2Digits = 4;     // digits per operand = accumulation levels
+constexpr int kOz2ListTiles = 8;  // tiles per CTA whose c / partner lists are staged in shared memory
+
+// digits of x (|x| < 2^31): x = d0 2^24 + d1 2^16 + d2 2^8 + d3 + r, every step exact
+__device__ __forceinline__ void oz2_digits(float x, float (&d)[kOz2Digits])
+{
+    float r = x;
+    d[0] = rint_small_mul(r, 0x1p-24f);
+    r = __fmaf_rn(-d[0], 0x1p24f, r);
+    d[1] = rint_small_mul(r, 0x1p-16f);
+    r = __fmaf_rn(-d[1], 0x1p16f, r);
+    d[2] = rint_small_mul(r, 0x1p-8f);
+    r = __fmaf_rn(-d[2], 0x1p8f, r);
+    d[3] = rint_small(r);
+}
 
 template <int NN>
 struct Oz2Shape {
@@ -361,17 +460,22 @@ struct Oz2Shape {
     static constexpr int CPT = 128 / NN;
     static constexpr int A_STAGE = KB * 128 * 128;   // one FP32 tile
     static constexpr int D_BYTES = 128 * 128;        // one digit tile (128 rows x 128 B)
+    static constexpr int D_SET = kOz2Digits * D_BYTES;
+    static constexpr int DSETS = (2 * A_STAGE + 2 * D_SET + kOz2Digits * N * 128 + 128 * (N + 1) * 4 + 8192 <=
+                                  227 * 1024) ? 2 : 1;   // digit buffers that fit
     static constexpr int B_BYTES = N * 128;
-    static constexpr int ACC = kOzLevels * N;        // TMEM columns per accumulator set
-    static constexpr int TMEM_COLS = 2 * ACC;        // 512 (n = 32) or 256 (n = 16)
+    static constexpr int ACC = kOz2Digits * N;           // TMEM columns per accumulator set
+    static constexpr int TMEM_COLS = 2 * ACC;
     static constexpr int S_LD = N + 1;
     static constexpr int OFF_A = 0;                                  // 2 stages
-    static constexpr int OFF_D = OFF_A + 2 * A_STAGE;                // kOzDigits digit tiles
-    static constexpr int OFF_B = OFF_D + kOzDigits * D_BYTES;        // kOzDigits B digit tiles
-    static constexpr int OFF_S = OFF_B + kOzDigits * B_BYTES;        // 128 x S_LD floats
-    static constexpr int OFF_E = OFF_S + 128 * S_LD * 4;             // eA[3][128], eB[N], sB[N]
-    static constexpr int OFF_BAR = OFF_E + (3 * 128 + N) * 4 + N * 4;
+    static constexpr int OFF_D = OFF_A + 2 * A_STAGE;                // DSETS digit sets
+    static constexpr int OFF_B = OFF_D + DSETS * D_SET;              // kOz2Digits B digit tiles
+    static constexpr int OFF_S = OFF_B + kOz2Digits * B_BYTES;       // 128 x S_LD floats
+    static constexpr int OFF_E = OFF_S + 128 * S_LD * 4;             // eA[4][128], sB[N]
+    static constexpr int OFF_L = OFF_E + 4 * 128 * 4 + N * 4;        // tile lists: c, partner
+    static constexpr int OFF_BAR = OFF_L + 2 * kOz2ListTiles * CPT * 4;
     static constexpr int SMEM = OFF_BAR + 16 * 8 + 1024;
+    static_assert(kOz2Digits * N <= ACC, "accumulator set");
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
@@ -386,14 +490,18 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
     unsigned char *Ds = sm + Sh::OFF_D;
     unsigned char *Bd = sm + Sh::OFF_B;
     float *S = reinterpret_cast<float *>(sm + Sh::OFF_S);
-    int *eA = reinterpret_cast<int *>(sm + Sh::OFF_E);      // [3][128]
-    float *sB = reinterpret_cast<float *>(eA + 3 * 128 + Sh::N);  // [N]
+    int *eA = reinterpret_cast<int *>(sm + Sh::OFF_E);           // [4][128]
+    float *sB = reinterpret_cast<float *>(eA + 4 * 128);         // [N]
+    int *lc = reinterpret_cast<int *>(sm + Sh::OFF_L);           // [kOz2ListTiles][CPT] c values
+    int *lp = lc + kOz2ListTiles * Sh::CPT;                      // partner slots
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Sh::OFF_BAR);
-    uint64_t *full_a = bar, *empty_a = bar + 2, *dig_full = bar + 4, *dig_empty = bar + 5, *acc_full = bar + 6,
-             *acc_empty = bar + 8;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 10);
+    uint64_t *full_a = bar, *empty_a = bar + 2, *dig_full = bar + 4, *dig_empty = bar + 6, *acc_full = bar + 8,
+             *acc_empty = bar + 10;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 12);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long n2 = (long long)NN * NN;
+    const int ntiles = 2 * s.gemm_tiles;
+    const int my_tiles = (ntiles - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -402,33 +510,30 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        mbar_init(&full_a[0], 1);
-        mbar_init(&full_a[1], 1);
-        mbar_init(&empty_a[0], 128);
-        mbar_init(&empty_a[1], 128);
-        mbar_init(dig_full, 128);
-        mbar_init(dig_empty, 1);
-        mbar_init(&acc_full[0], 1);
-        mbar_init(&acc_full[1], 1);
-        mbar_init(&acc_empty[0], 128);
-        mbar_init(&acc_empty[1], 128);
+        for (int q = 0; q < 2; ++q) {
+            mbar_init(&full_a[q], 1);
+            mbar_init(&empty_a[q], 256);
+            mbar_init(&dig_full[q], 256);
+            mbar_init(&dig_empty[q], 1);
+            mbar_init(&acc_full[q], 1);
+            mbar_init(&acc_empty[q], 256);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // digit tiles start at zero (the n = 16 rows fill half of each 128-byte row);
-    // the B digit tiles and row scales of h were written by k_prep (h_digits)
-    for (int i = tid; i < kOzDigits * Sh::D_BYTES / 16; i += blockDim.x)
-        reinterpret_cast<uint4 *>(Ds)[i] = make_uint4(0, 0, 0, 0);
-    const uint4 *bsrc = reinterpret_cast<const uint4 *>(s.d.ozb);
-    for (int i = tid; i < kOzDigits * Sh::B_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4 *>(Bd)[i] = bsrc[i];
-    const float *sbsrc = reinterpret_cast<const float *>(s.d.ozb + kOzDigits * Sh::B_BYTES);
-    for (int j = tid; j < Sh::N; j += blockDim.x) sB[j] = sbsrc[j];
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    // c values and partner slots of this CTA's first tiles (independent loads)
+    for (int x = tid; x < min(my_tiles, kOz2ListTiles) * Sh::CPT; x += blockDim.x) {
+        const int g = (blockIdx.x + (x / Sh::CPT) * gridDim.x) % s.gemm_tiles;
+        lc[x] = s.gemm_c[g * Sh::CPT + x % Sh::CPT];
+        lp[x] = s.gemm_partner[g * Sh::CPT + x % Sh::CPT];
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-    const int ntiles = 2 * s.gemm_tiles;
-    const int my_tiles = (ntiles - int(blockIdx.x) + int(gridDim.x) - 1) / int(gridDim.x);
+    auto tile_c = [&](int i, int g, int slot) { return i < kOz2ListTiles ? lc[i * Sh::CPT + slot] : s.gemm_c[g * Sh::CPT + slot]; };
+    auto tile_p = [&](int i, int g, int slot) {
+        return i < kOz2ListTiles ? lp[i * Sh::CPT + slot] : s.gemm_partner[g * Sh::CPT + slot];
+    };
     bool ok = true;
 
     if (warp == 0) {
@@ -444,7 +549,7 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
                 }
                 mbar_expect_tx(&full_a[sa], Sh::A_STAGE);
                 for (int slot = 0; slot < Sh::CPT; ++slot) {
-                    const int c = s.gemm_c[g * Sh::CPT + slot];
+                    const int c = tile_c(i, g, slot);
                     for (int kb = 0; kb < Sh::KB; ++kb)
                         tma_load_4d(As + sa * Sh::A_STAGE + kb * 128 * 128 + slot * NN * 128, &tmap, &full_a[sa],
                                     kb * 32, c, 0, t);
@@ -457,143 +562,184 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
                 for (int i = (issued >= 2 ? issued - 2 : 0); i < issued; ++i) mbar_wait(&full_a[i & 1], (i >> 1) & 1);
             }
         }
-    } else if (warp == 1) {
-        // ---- MMA issuer
-        if (lane == 0) {
-            const uint32_t idesc = umma_idesc_bf16(Sh::N);
-            const uint32_t ab = smem_u32(Ds), bb = smem_u32(Bd);
-            int done = 0;
+    } else {
+        // warps 1-17: digit buffers start at zero (the n = 16 rows fill half of
+        // each 128-byte row); B digit tiles and row scales of h from k_prep
+        for (int i = tid - 32; i < Sh::DSETS * Sh::D_SET / 16; i += blockDim.x - 32)
+            reinterpret_cast<uint4 *>(Ds)[i] = make_uint4(0, 0, 0, 0);
+        const uint4 *bsrc = reinterpret_cast<const uint4 *>(s.d.ozb);
+        for (int i = tid - 32; i < kOz2Digits * Sh::B_BYTES / 16; i += blockDim.x - 32)
+            reinterpret_cast<uint4 *>(Bd)[i] = bsrc[i];
+        const float *sbsrc = reinterpret_cast<const float *>(s.d.ozb + kOz2Digits * Sh::B_BYTES);
+        for (int j = tid - 32; j < Sh::N; j += blockDim.x - 32) sB[j] = sbsrc[j];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        named_sync(2, kOz2Threads - 32);
+        tc_fence_after();
+
+        if (warp == 1) {
+            // ---- MMA issuer
+            if (lane == 0) {
+                const uint32_t idesc = umma_idesc_bf16(Sh::N);
+                const uint32_t bb = smem_u32(Bd);
+                int done = 0;
+                for (int i = 0; i < my_tiles; ++i) {
+                    const int b = i & 1, db = i % Sh::DSETS, du = i / Sh::DSETS;
+                    if (!mbar_wait(&dig_full[db], du & 1) ||
+                        (i >= 2 && !mbar_wait(&acc_empty[b], ((i - 2) >> 1) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t ab = smem_u32(Ds + db * Sh::D_SET);
+                    const uint32_t acc0 = tmem + b * Sh::ACC;
+                    for (int L = 0; L < kOz2Digits; ++L) {
+                        uint32_t acc = 0;
+                        for (int ii = 0; ii <= L; ++ii) {
+                            const int jj = L - ii;
+                            for (int ks = 0; ks < Sh::KS; ++ks) {
+                                umma_bf16(acc0 + L * Sh::N, umma_desc_sw128(ab + ii * Sh::D_BYTES + ks * 32),
+                                          umma_desc_sw128(bb + jj * Sh::B_BYTES + ks * 32), idesc, acc);
+                                acc = 1;
+                            }
+                        }
+                    }
+                    umma_commit(&acc_full[b]);
+                    umma_commit(&dig_empty[db]);
+                    done = i + 1;
+                }
+                if (!ok) {
+                    atomicExch(s.err, 5);
+                    if (done > 0)  // the last products have landed
+                        mbar_wait(&dig_empty[(done - 1) % Sh::DSETS], ((done - 1) / Sh::DSETS) & 1);
+                }
+            }
+        } else if (warp < 10) {
+            // ---- digit split: threads (2m, 2m+1) share row m, each half of its K values
+            const int dt = tid - 64;
+            const int m = dt >> 1, half = dt & 1;
+            const int sw = m & 7;
+            constexpr int HF = Sh::KF / 2;   // FP32 values per thread
+            constexpr int HC = Sh::DC / 2;   // digit chunks per thread
+            for (int i = 0; i < my_tiles; ++i) {
+                const int sa = i & 1, db = i % Sh::DSETS, du = i / Sh::DSETS;
+                bool w = mbar_wait(&full_a[sa], (i >> 1) & 1) &&
+                         (i < Sh::DSETS || mbar_wait(&dig_empty[db], (du - 1) & 1));
+                if (!__all_sync(0xffffffffu, w)) {  // warp-uniform exit (the pair shuffle below)
+                    ok = false;
+                    break;
+                }
+                float v[HF];
+                const unsigned char *row = As + sa * Sh::A_STAGE + m * 128;
+#pragma unroll
+                for (int q4 = 0; q4 < HF / 4; ++q4) {
+                    const int f = half * HF + 4 * q4;            // first FP32 index of this 16-byte chunk
+                    const int kb = f >> 5, j = (f & 31) >> 2;
+                    const float4 q = *reinterpret_cast<const float4 *>(row + kb * 128 * 128 + ((j ^ sw) << 4));
+                    v[4 * q4 + 0] = q.x;
+                    v[4 * q4 + 1] = q.y;
+                    v[4 * q4 + 2] = q.z;
+                    v[4 * q4 + 3] = q.w;
+                }
+                mbar_arrive(&empty_a[sa]);
+                float mx = 0.f;
+#pragma unroll
+                for (int x = 0; x < HF; ++x) mx = fmaxf(mx, fabsf(v[x]));
+                mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+                const int e = (mx > 0.f) ? max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, -100) : 0;
+                if (half == 0) eA[(i & 3) * 128 + m] = e;
+                const float sc = pow2f(30 - e);
+                unsigned char *Dst = Ds + db * Sh::D_SET + m * 128;
+#pragma unroll
+                for (int hc = 0; hc < HC; ++hc) {
+                    const int ch = half * HC + hc;
+                    uint32_t w4[kOz2Digits][4];
+#pragma unroll
+                    for (int pr = 0; pr < 4; ++pr) {
+                        float d0[kOz2Digits], d1[kOz2Digits];
+                        oz2_digits(v[hc * 8 + 2 * pr] * sc, d0);
+                        oz2_digits(v[hc * 8 + 2 * pr + 1] * sc, d1);
+#pragma unroll
+                        for (int q = 0; q < kOz2Digits; ++q) w4[q][pr] = bf16x2_of_ints(d0[q], d1[q]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < kOz2Digits; ++q)
+                        *reinterpret_cast<uint4 *>(Dst + q * Sh::D_BYTES + ((ch ^ sw) << 4)) =
+                            make_uint4(w4[q][0], w4[q][1], w4[q][2], w4[q][3]);
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(&dig_full[db]);
+            }
+            if (!ok) atomicExch(s.err, 6);
+        } else {
+            // ---- epilogue: warp (quadrant q, part h) reads TMEM lanes 32q..32q+31,
+            // columns h*NN .. h*NN+NN-1 of every level
+            const int quad = warp & 3, hp = (warp - 10) >> 2;
+            const int row = quad * 32 + lane;
+            const int et = tid - 320;  // 0..255
+            __shared__ int vote[8];
+            constexpr int LB = (NN == 32) ? 2 : kOz2Digits;  // levels per TMEM load batch (registers)
             for (int i = 0; i < my_tiles; ++i) {
                 const int b = i & 1;
-                if (!mbar_wait(dig_full, i & 1) || (i >= 2 && !mbar_wait(&acc_empty[b], ((i - 2) >> 1) & 1))) {
+                const int tile = blockIdx.x + i * gridDim.x;
+                const int t = tile / s.gemm_tiles, g = tile % s.gemm_tiles;
+                // the eight epilogue warps leave together (they share a named barrier)
+                const bool w = __all_sync(0xffffffffu, mbar_wait(&acc_full[b], (i >> 1) & 1));
+                if (lane == 0) vote[warp - 10] = w ? 1 : 0;
+                named_sync(1, 256);
+                bool all = true;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) all = all && vote[q];
+                if (!all) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t acc0 = tmem + b * Sh::ACC;
-                for (int L = 0; L < kOzLevels; ++L) {
-                    uint32_t acc = 0;
-                    for (int ii = 0; ii <= L; ++ii) {
-                        const int jj = L - ii;
-                        for (int ks = 0; ks < Sh::KS; ++ks) {
-                            umma_bf16(acc0 + L * Sh::N, umma_desc_sw128(ab + ii * Sh::D_BYTES + ks * 32),
-                                      umma_desc_sw128(bb + jj * Sh::B_BYTES + ks * 32), idesc, acc);
-                            acc = 1;
+                const float sa = pow2f(eA[(i & 3) * 128 + row] - 6);
+                const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * Sh::ACC + hp * NN;
+                float acc[NN];
+#pragma unroll
+                for (int x = 0; x < NN; ++x) acc[x] = 0.f;
+                // sum_L 2^(-8L) P_L, smallest level first (FP32, round to nearest);
+                // up to LB levels loaded per wait
+#pragma unroll
+                for (int L0 = kOz2Digits - 1; L0 >= 0; L0 -= LB) {
+                    float wv[LB][NN];
+#pragma unroll
+                    for (int l = 0; l < LB; ++l)
+                        if (L0 - l >= 0) tmem_ldw_nowait<NN>(ta + (L0 - l) * Sh::N, wv[l]);
+#pragma unroll
+                    for (int l = 0; l < LB; ++l)
+                        if (L0 - l >= 0) tmem_wait_ld(wv[l]);
+#pragma unroll
+                    for (int l = 0; l < LB; ++l)
+                        if (L0 - l >= 0) {
+#pragma unroll
+                            for (int x = 0; x < NN; ++x) acc[x] = fmaf(acc[x], 0x1p-8f, wv[l][x]);
                         }
+                }
+#pragma unroll
+                for (int x = 0; x < NN; ++x) S[row * Sh::S_LD + hp * NN + x] = acc[x] * sa * sB[hp * NN + x];
+                tc_fence_before();
+                mbar_arrive(&acc_empty[b]);
+                named_sync(1, 256);
+                float *Wg = s.W + t * 2 * s.n4;
+#pragma unroll 2
+                for (int sp = 0; sp < Sh::CPT * 2; ++sp) {
+                    const int slot = sp >> 1, part = sp & 1;
+                    const int ps = tile_p(i, g, slot);
+                    float *Wrow = Wg + ((long long)tile_c(i, g, slot) * 2 + part) * n2;
+#pragma unroll
+                    for (int r = et; r < NN * NN; r += 256) {
+                        const int mu1 = r % NN, mu2 = r / NN;
+                        Wrow[r] = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] +
+                                  S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
                     }
                 }
-                umma_commit(&acc_full[b]);
-                umma_commit(dig_empty);
-                done = i + 1;
+                named_sync(1, 256);
             }
-            if (!ok) {
-                atomicExch(s.err, 5);
-                if (done > 0) mbar_wait(dig_empty, (done - 1) & 1);  // the last products have landed
-            }
+            if (!ok) atomicExch(s.err, 7);
         }
-    } else if (warp < 6) {
-        // ---- digit split: thread -> row m
-        const int m = tid - 64;
-        const int sw = m & 7;
-        for (int i = 0; i < my_tiles; ++i) {
-            const int sa = i & 1;
-            if (!mbar_wait(&full_a[sa], (i >> 1) & 1) || (i >= 1 && !mbar_wait(dig_empty, (i - 1) & 1))) {
-                ok = false;
-                break;
-            }
-            float v[Sh::KF];
-            const unsigned char *row = As + sa * Sh::A_STAGE + m * 128;
-#pragma unroll
-            for (int kb = 0; kb < Sh::KB; ++kb)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const float4 q = *reinterpret_cast<const float4 *>(row + kb * 128 * 128 + ((j ^ sw) << 4));
-                    v[kb * 32 + 4 * j + 0] = q.x;
-                    v[kb * 32 + 4 * j + 1] = q.y;
-                    v[kb * 32 + 4 * j + 2] = q.z;
-                    v[kb * 32 + 4 * j + 3] = q.w;
-                }
-            mbar_arrive(&empty_a[sa]);
-            float mx = 0.f;
-#pragma unroll
-            for (int x = 0; x < Sh::KF; ++x) mx = fmaxf(mx, fabsf(v[x]));
-            const int e = (mx > 0.f) ? max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, -100) : 0;
-            eA[(i % 3) * 128 + m] = e;
-            const float sc = pow2f(20 - e);
-#pragma unroll
-            for (int ch = 0; ch < Sh::DC; ++ch) {
-                uint32_t w[kOzDigits][4];
-#pragma unroll
-                for (int pr = 0; pr < 4; ++pr) {
-                    float d0[kOzDigits], d1[kOzDigits];
-                    oz_digits(v[ch * 8 + 2 * pr] * sc, d0);
-                    oz_digits(v[ch * 8 + 2 * pr + 1] * sc, d1);
-#pragma unroll
-                    for (int q = 0; q < kOzDigits; ++q) {
-                        const __nv_bfloat162 p2 = __floats2bfloat162_rn(d0[q], d1[q]);
-                        w[q][pr] = *reinterpret_cast<const uint32_t *>(&p2);
-                    }
-                }
-#pragma unroll
-                for (int q = 0; q < kOzDigits; ++q)
-                    *reinterpret_cast<uint4 *>(Ds + q * Sh::D_BYTES + m * 128 + ((ch ^ sw) << 4)) =
-                        make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
-            }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(dig_full);
-        }
-        if (!ok) atomicExch(s.err, 6);
-    } else {
-        // ---- epilogue: warp quadrant q reads TMEM lanes 32q..32q+31
-        const int quad = warp & 3;
-        const int row = quad * 32 + lane;
-        const int et = tid - 192;  // 0..127
-        for (int i = 0; i < my_tiles; ++i) {
-            const int b = i & 1;
-            const int tile = blockIdx.x + i * gridDim.x;
-            const int t = tile / s.gemm_tiles, g = tile % s.gemm_tiles;
-            if (!mbar_wait(&acc_full[b], (i >> 1) & 1)) {
-                ok = false;
-                break;
-            }
-            tc_fence_after();
-            const float sa = pow2f(eA[(i % 3) * 128 + row] - 6);
-            const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * Sh::ACC;
-#pragma unroll
-            for (int cb = 0; cb < Sh::N; cb += 32) {
-                float acc[32];
-#pragma unroll
-                for (int x = 0; x < 32; ++x) acc[x] = 0.f;
-#pragma unroll
-                for (int L = kOzLevels - 1; L >= 0; --L) {
-                    float w[32];
-                    tmem_ld32(ta + L * Sh::N + cb, w);
-                    // sum_L 2^(-7L) P_L, smallest level first (FP32, round to nearest)
-#pragma unroll
-                    for (int x = 0; x < 32; ++x) acc[x] = fmaf(acc[x], 0x1p-7f, w[x]);
-                }
-#pragma unroll
-                for (int x = 0; x < 32; ++x) S[row * Sh::S_LD + cb + x] = acc[x] * sa * sB[cb + x];
-            }
-            tc_fence_before();
-            mbar_arrive(&acc_empty[b]);
-            named_sync(1, 128);
-            float *Wg = s.W + t * 2 * s.n4;
-#pragma unroll 1
-            for (int sp = 0; sp < Sh::CPT * 2; ++sp) {
-                const int slot = sp >> 1, part = sp & 1;
-                const int ps = s.gemm_partner[g * Sh::CPT + slot];
-                float *Wrow = Wg + ((long long)s.gemm_c[g * Sh::CPT + slot] * 2 + part) * n2;
-#pragma unroll 4
-                for (int r = et; r < NN * NN; r += 128) {
-                    const int mu1 = r % NN, mu2 = r / NN;
-                    Wrow[r] = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] +
-                              S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
-                }
-            }
-            named_sync(1, 128);
-        }
-        if (!ok) atomicExch(s.err, 7);
     }
     tc_fence_before();
     __syncthreads();

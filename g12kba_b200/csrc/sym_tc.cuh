@@ -52,13 +52,27 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
     return done != 0;
 }
 
+// one hardware-suspended wait for phase `parity` (returns false when the
+// hardware's time window ends first; the thread wakes as soon as the phase completes)
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
 // bounded wait on phase `parity`; false when the cycle budget runs out
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 {
     const long long t0 = clock64();
-    while (!mbar_test(bar, parity)) {
+    while (!mbar_try(bar, parity)) {
         if (clock64() - t0 > kWaitCycles) return false;
-        __nanosleep(20);
     }
     return true;
 }

@@ -42,8 +42,8 @@ enum g12_vlaw { G12_VLAW_EXP = 0, G12_VLAW_INV = 1 };
 enum g12_precision {
     G12_PREC_FP64 = 0,    /* plain FP64 path (parity with the reference) */
     G12_PREC_TF32X3 = 1,  /* two-body commutator on tcgen05 kind::tf32: 2 tf32 pieces, 3 products */
-    G12_PREC_BF16OZ = 2,  /* tcgen05 kind::f16: exact 7-bit integer digits in bf16 (4 per operand,
-                             10 products), unbiased; the accurate mixed mode */
+    G12_PREC_BF16OZ = 2,  /* tcgen05 kind::f16: exact 8-bit integer digits in bf16 (4 per operand,
+                             10 products, exact FP32 partial sums), unbiased; the accurate mixed mode */
     G12_PREC_FP32 = 3,    /* symmetric engine with an FP32 CUDA-core contraction (checker) */
     G12_PREC_TF32X6 = 4   /* tcgen05 kind::tf32: 3 tf32 pieces per operand, 6 products */
 };
