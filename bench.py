@@ -46,13 +46,21 @@ CONFIG = {"workload": "HF-GKBA GW, Hubbard chain Ns=16 Nb=2 (n=32), EHM w(r)=U/(
 EVICT_BYTES = 160 << 20
 
 
-# DRAM bytes (read + write) per launch of the top kernels, from one
-# `ncu --set full` capture each (profiles/ summaries name the command).
+# DRAM bytes (read + write) per launch of the top kernels at n = 32, from one
+# `ncu --set full` capture each (the profiles/ summaries give the command).
 TOP_KERNEL_DRAM_BYTES = {
-    "k_sym_gemm_oz": 16906496.0,
-    "k_sym_epi": 55267328.0,
+    "k_sym_gemm_oz2": 16863232.0,
+    "k_sym_epi": 37610752.0,
     "k_apply<cols+epilogue>": 95704832.0,
 }
+
+# Algorithmic HBM bytes per launch in units of n^4 (both G2 tensors):
+#   k_sym_gemm_*: read the FP32 stage input (16 n^4), write W (16 n^4);
+#   k_sym_epi:    read W (16), Yc (16.5), Ac (24.75 stage average), write the next
+#                 FP32 input (16) and, at the last stage, Yc (16.5 / 4): 77.4 n^4.
+ALG_BYTES_N4 = {"k_sym_gemm_oz2": 32.0, "k_sym_gemm_oz": 32.0, "k_sym_gemm_tc": 32.0, "k_sym_gemm_simt": 32.0,
+                "k_sym_epi": 77.4}
+MIXED_STEP_BYTES_N4 = 4 * (32.0 + 77.4)
 
 
 def log(*a):
@@ -372,9 +380,7 @@ def main():
     top_ms = kt[top][0]
     fp64_peak = g12.fp64_peak_tflops(local)
     if mixed:
-        # k_sym_gemm_*: reads the FP32 stage input, writes W (FP32), both tensors:
-        # 2 x n^4 x (8 + 8) bytes per launch
-        bytes_alg = 32.0 * n ** 4 if "gemm" in top else 40.0 * n ** 4
+        bytes_alg = ALG_BYTES_N4.get(top, 0.0) * n ** 4
         roofline = {"bound": "hbm", "kernel": top, "achieved": bytes_alg / (top_ms * 1e-3) / 1e9, "peak": hbm,
                     "unit": "GB/s", "frac": bytes_alg / (top_ms * 1e-3) / 1e9 / hbm,
                     "traffic": TOP_KERNEL_DRAM_BYTES.get(top), "algorithmic_bytes": bytes_alg,
@@ -386,8 +392,9 @@ def main():
                     "traffic": TOP_KERNEL_DRAM_BYTES.get(top),
                     "peak_source": "measured FP64 FMA probe (g12_fp64_peak_tflops) on this GPU"}
     # whole step against the per-step figure 640 n^4 bytes (FP64 state passes)
-    step_roofline = {"bytes_per_step": 640.0 * n ** 4, "achieved_gbs": 640.0 * n ** 4 * value / world / 1e9,
-                     "frac_of_hbm": 640.0 * n ** 4 * value / world / 1e9 / hbm,
+    mb = MIXED_STEP_BYTES_N4 * n ** 4 if mixed else 640.0 * n ** 4
+    step_roofline = {"bytes_per_step_fp64_state": 640.0 * n ** 4, "bytes_per_step_this_engine": mb,
+                     "achieved_gbs": mb * value / world / 1e9, "frac_of_hbm": mb * value / world / 1e9 / hbm,
                      "flops_per_step": 256.0 * n ** 5, "fp64_peak_tflops": fp64_peak}
     if mixed:
         mx.close()

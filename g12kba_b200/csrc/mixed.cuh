@@ -222,7 +222,7 @@ inline int mixed_kernel_kinds(const MixedState &) { return 2; }
 
 inline const char *mixed_kernel_name(const MixedState &m, int q)
 {
-    if (q == 0) return m.oz ? "k_sym_gemm_oz" : (m.tc ? "k_sym_gemm_tc" : "k_sym_gemm_simt");
+    if (q == 0) return m.oz2 ? "k_sym_gemm_oz2" : m.oz ? "k_sym_gemm_oz" : (m.tc ? "k_sym_gemm_tc" : "k_sym_gemm_simt");
     if (q == 1) return "k_sym_epi";
     return "";
 }
