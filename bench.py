@@ -195,17 +195,24 @@ def run_reference_arm(args):
     }))
 
 
-def ensemble_measure(g12, local, steps=20, warmup=3, sample=16):
-    """256 uneven systems (n = 4..24) in one batch (FP64 engine) against the same
-    systems run one context at a time (a seeded sample of them, scaled).  The
-    ensemble's state (about 2 GB) is far larger than L2."""
+def ensemble_measure(g12, local, rank=0, world=1, pg=None, steps=20, warmup=3, sample=16):
+    """256 uneven systems (n = 4..24) in one batch per GPU (FP64 engine; with N
+    ranks the systems are partitioned by cost, no communication while they
+    propagate) against the same systems run one context at a time (a seeded
+    sample of them on rank 0, scaled).  The ensemble's state (about 2 GB) is
+    far larger than L2."""
+    from g12kba_b200 import ensemble
     ps = g12.ensemble_params(256)
-    with g12.Batch(ps, "fp64", local) as b:
-        for i, p in enumerate(ps):
+    mine = [ps[i] for i in ensemble.partition(ps, world)[rank]]
+    with g12.Batch(mine, "fp64", local) as b:
+        for i, p in enumerate(mine):
             b.set_state(i, g12.make_G0(p))
         b.propagate(warmup)
+        barrier(pg)
         b.propagate(steps)
-        ms = b.last_device_ms
+        ms = allmax(pg, b.last_device_ms)
+    if rank != 0:
+        return None
     rng = np.random.default_rng(1)
     idx = rng.choice(len(ps), size=sample, replace=False)
     seq_ms = 0.0
@@ -217,12 +224,13 @@ def ensemble_measure(g12, local, steps=20, warmup=3, sample=16):
             seq_ms += ctx.last_device_ms
     seq_total = seq_ms * len(ps) / sample
     ns = [p.n for p in ps]
-    return {"systems": len(ps), "n_values": sorted(set(ns)), "ensemble_steps_per_s": steps / (ms / 1e3),
-            "system_steps_per_s": len(ps) * steps / (ms / 1e3),
-            "one_context_at_a_time_steps_per_s": steps / (seq_total / 1e3),
+    return {"systems": len(ps), "n_values": sorted(set(ns)), "ranks": world,
+            "ensemble_steps_per_s": steps / (ms / 1e3), "system_steps_per_s": len(ps) * steps / (ms / 1e3),
+            "one_context_at_a_time_steps_per_s_one_gpu": steps / (seq_total / 1e3),
             "speedup_vs_one_context_at_a_time": seq_total / ms,
-            "note": f"{steps} timed steps after {warmup}; sequential figure from {sample} sampled systems x "
-                    f"{len(ps)}/{sample}; from G0 with G2 = 0 (step cost does not depend on the state)"}
+            "note": f"{steps} timed steps after {warmup}, max device time over ranks; sequential figure from "
+                    f"{sample} sampled systems x {len(ps)}/{sample} on one GPU; from G0 with G2 = 0 (step cost "
+                    f"does not depend on the state)"}
 
 
 def learned_measure(g12, local, ntrain=64, ntest=8, T=3000, P=400, train_steps=8000, judge_every=200):
@@ -401,8 +409,8 @@ def main():
     fp.close()
 
     ensemble = None
-    if rank == 0 and not args.no_ensemble:
-        ensemble = ensemble_measure(g12, local)
+    if not args.no_ensemble:
+        ensemble = ensemble_measure(g12, local, rank, world, pg)
 
     learned = None
     if rank == 0 and not args.no_learned:
