@@ -270,6 +270,11 @@ def learned_measure(g12, local, ntrain=64, ntest=8, T=3000, P=400, train_steps=8
             ctx.propagate_dipole(400)
             rk[prec] = 400 / (ctx.last_device_ms / 1e3)
     net_per_traj = (Tr - P) / (net_ms / 1e3)  # snapshots per second per trajectory (all rolled out together)
+    # the non-learned comparator: exact DMD fitted on the same RK4 prefixes
+    t2 = time.perf_counter()
+    dmd = L.dmd_rollout(fte[:, :P], Tr, window=min(P - 1, 400))
+    dmd_s = time.perf_counter() - t2
+    derr = L.running_errors(dmd, truth, 16, P - 1)
     dt = 0.01
 
     def covered(h):
@@ -288,6 +293,11 @@ def learned_measure(g12, local, ntrain=64, ntest=8, T=3000, P=400, train_steps=8
         "plain_rk4_simulated_time_per_s": {k: dt * v for k, v in rk.items()},
         "horizon_steps_median_err_le_1e-3": h3, "horizon_steps_median_err_le_1e-2": h2,
         "judge_every_steps": judge_every,
+        "dmd_comparator": {"horizon_steps_median_err_le_1e-3": L.horizon(derr, 1e-3),
+                           "horizon_steps_median_err_le_1e-2": L.horizon(derr, 1e-2),
+                           "median_err_after_200_steps": float(np.median(derr[:, min(199, derr.shape[1] - 1)])),
+                           "host_seconds": dmd_s, "window": min(P - 1, 400)},
+        "network_median_err_after_200_steps": float(np.median(errs[:, min(199, errs.shape[1] - 1)])),
         "judge_checkpoint_median_err": {int(c): float(np.median(ce[:, i])) for i, c in enumerate(cks[:10])},
         "simulated_time_per_s_within_1e-3": covered(h3),
         "speedup_vs_plain_fp64_within_1e-3": covered(h3) / (dt * rk["fp64"]),

@@ -82,6 +82,7 @@ def lib():
         L.g12_rk_iterations.argtypes = [C.POINTER(Params)]
         L.g12_make_G0.argtypes = [C.POINTER(Params), C.c_int32, _dp]
         L.g12_dipole.argtypes = [_dp, C.c_int64, C.c_int32, _dp]
+        L.g12_particle_number.argtypes = [_dp, C.c_int64, C.c_int32, _dp]
         L.g12_write_cfile2D.argtypes = [C.c_char_p, _dp, C.c_int64, C.c_int32]
         L.g12_write_rfile.argtypes = [C.c_char_p, _dp, C.c_int64]
         L.g12_create.argtypes = [C.POINTER(Params), C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
@@ -213,6 +214,16 @@ def dipole(traj):
     n = int(round(np.sqrt(traj[0].size)))
     out = np.zeros(T)
     _check(lib().g12_dipole(_ptr(traj), T, n, _ptr(out)))
+    return out
+
+
+def particle_number(traj):
+    """N = 2 Tr Im G1 per snapshot of traj [T, n, n] (conserved by the equations)."""
+    traj = np.ascontiguousarray(traj, np.complex128)
+    if traj.ndim == 2:
+        traj = traj[None]
+    out = np.zeros(traj.shape[0])
+    _check(lib().g12_particle_number(_ptr(traj), traj.shape[0], traj.shape[-1], _ptr(out)))
     return out
 
 

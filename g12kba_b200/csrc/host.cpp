@@ -452,6 +452,20 @@ extern "C" int g12_dipole(const double *traj, int64_t T, int32_t n, double *p_ou
     return G12_OK;
 }
 
+extern "C" int g12_particle_number(const double *traj, int64_t T, int32_t n, double *N_out)
+{
+    // N = 2 Tr Im G1 (two spin projections of rho = -i G1); the G1-G2
+    // equations conserve it exactly (RK_solver.h:101 guards its site-0 part)
+    if (!traj || !N_out || n < 1) return G12_ERR_INVALID;
+    const int64_t NN = int64_t(n) * n;
+    for (int64_t t = 0; t < T; ++t) {
+        double s = 0.0;
+        for (int i = 0; i < n; ++i) s += traj[2 * (t * NN + int64_t(i) * (n + 1)) + 1];
+        N_out[t] = 2.0 * s;
+    }
+    return G12_OK;
+}
+
 namespace {
 
 // std::ostream << double with default flags and precision 6 == "%.6g".

@@ -316,3 +316,30 @@ def running_errors(pred, truth, n, t0):
     pt = dipole_from_features(np.asarray(truth), n)
     amp = np.maximum(np.max(np.abs(pt), axis=1), 1e-12)
     return np.maximum.accumulate(np.abs(pr[:, t0 + 1:] - pt[:, t0 + 1:]) / amp[:, None], axis=1)
+
+
+def dmd_rollout(prefix, total, window=400, rank=None, tol=1e-10):
+    """Exact dynamic mode decomposition (Tu, Rowley, Luchtenburg, Brunton, Kutz,
+    J. Comput. Dyn. 1, 2014) as the non-learned comparator: fit the linear map
+    x_{s+1} = A x_s on the last `window` snapshots of each trajectory's exact
+    prefix (numpy float64, host), in the basis of the singular vectors above
+    `tol` (relative) or the first `rank`, and iterate it to `total` snapshots.
+    prefix: [ntraj][t0+1][F] (numpy or torch); returns numpy [ntraj][total][F]."""
+    pre = prefix.detach().cpu().numpy() if hasattr(prefix, "detach") else np.asarray(prefix)
+    pre = pre.astype(np.float64)
+    ntraj, t1, F = pre.shape
+    out = np.zeros((ntraj, total, F))
+    out[:, :t1] = pre
+    for b in range(ntraj):
+        Xw = pre[b, max(0, t1 - window - 1):t1].T  # F x (w+1)
+        X, Y = Xw[:, :-1], Xw[:, 1:]
+        U, sv, Vt = np.linalg.svd(X, full_matrices=False)
+        r = int(np.sum(sv > tol * sv[0])) if rank is None else min(rank, sv.size)
+        U, sv, Vt = U[:, :r], sv[:r], Vt[:r]
+        At = U.T @ Y @ Vt.T / sv  # r x r, the map in the basis U
+        z = U.T @ pre[b, -1]
+        res = pre[b, -1] - U @ z  # the part outside the basis, held fixed
+        for s_ in range(t1, total):
+            z = At @ z
+            out[b, s_] = U @ z + res
+    return out

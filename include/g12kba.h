@@ -97,6 +97,11 @@ int g12_make_G0(const g12_params *p, int32_t p_number, double *G1_out);
 /* dipole.h:25-32 over T snapshots (host). */
 int g12_dipole(const double *traj, int64_t T, int32_t n, double *p_out);
 
+/* Particle number N = 2 Tr Im G1 per snapshot (host).  No counterpart in the
+ * reference, which only guards the site-0 density (RK_solver.h:101-110); the
+ * equations conserve N exactly, so it checks a propagation. */
+int g12_particle_number(const double *traj, int64_t T, int32_t n, double *N_out);
+
 /* write_to_file.h:52-69 (real_/imag_<name>) and :26-34; std::ostream default
  * formatting (6 significant digits). */
 int g12_write_cfile2D(const char *name, const double *traj, int64_t T, int32_t n2);

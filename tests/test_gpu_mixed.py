@@ -100,3 +100,17 @@ def test_l2_eviction_changes_nothing(g12, prec):
     assert np.array_equal(out[0][0], out[1][0])
     for a, b in zip(out[0][1], out[1][1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("bf16oz", 1e-9)])
+def test_particle_number_conserved(g12, prec, tol):
+    """2 Tr Im G1 is a linear invariant of the equations, so RK4 keeps it."""
+    cfg = Config(Ns=8, Nb=2, Nq=3, time_steps=300, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, vlaw="inv",
+                 q_type="pulse", quench_strength=2.0, quench_rate=2, quench_on_midpoint=1, quench_off_midpoint=2,
+                 AS_rate=0.3, AS_midpoint=2.0)
+    p = params_of(g12, cfg)
+    p.quench_gate = 0.0
+    traj, rc, _ = _run(g12, p, prec, g12.make_G0(p), 300)
+    assert rc == 0
+    N = g12.particle_number(traj)
+    assert np.max(np.abs(N - N[0])) <= tol * abs(N[0]), np.max(np.abs(N - N[0]))

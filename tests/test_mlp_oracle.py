@@ -66,3 +66,32 @@ def test_oracle_windows_layout():
     assert np.allclose(X[0, :4], (feat[1, 7] - feat[1, 10]) / 2.0)
     assert np.allclose(X[0, 12:], (feat[1, 10] - mean) / 3.0)
     assert np.allclose(Y[0, 4:8], (feat[1, 12] - feat[1, 10]) / 5.0)
+
+
+def test_dmd_reproduces_a_linear_system():
+    """DMD on snapshots of x_{s+1} = A x_s (damped rotations) continues them exactly."""
+    from g12kba_b200 import learned
+    rng = np.random.default_rng(4)
+    F, r = 40, 6
+    Q, _ = np.linalg.qr(rng.standard_normal((F, F)))
+    blocks = np.zeros((F, F))
+    for k in range(r // 2):
+        th, rho = 0.05 * (k + 1), 0.999 - 0.001 * k
+        blocks[2 * k:2 * k + 2, 2 * k:2 * k + 2] = rho * np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]])
+    A = Q @ blocks @ Q.T
+    x = Q[:, :r] @ rng.standard_normal(r)
+    traj = [x]
+    for _ in range(499):
+        traj.append(A @ traj[-1])
+    traj = np.array(traj)[None]
+    pred = learned.dmd_rollout(traj[:, :200], 500, window=150)
+    assert np.max(np.abs(pred[0, 200:] - traj[0, 200:])) <= 1e-8 * np.max(np.abs(traj))
+
+
+def test_particle_number_of_a_trajectory(g12):
+    rng = np.random.default_rng(5)
+    n = 6
+    a = rng.standard_normal((3, n, n)) + 1j * rng.standard_normal((3, n, n))
+    G1 = 1j * (a + np.conj(np.swapaxes(a, -1, -2))) / 2
+    N = g12.particle_number(G1)
+    assert np.allclose(N, 2 * np.trace(G1.imag, axis1=1, axis2=2))
