@@ -158,6 +158,7 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
         const int m = abs(s1 - s2);
         return (m >= 1 && m <= d.nv) ? U * d.law[m - 1] : 0.0;
     };
+    bool fused = false;  // RK bookkeeping done inside the K loop
     if constexpr (NN >= kTB) {
         // n >= 32: every 32 x 32 tile has one mu2 (rows) and one nu2 (columns),
         // so the site weights, Rt, the Pi factor Q and (for xx) the three-G1
@@ -189,6 +190,8 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
         }
         __syncthreads();
         const double2 g22 = Gs[mu2 * GLD + nu2];
+        fused = !diag && !d.debug;
+        double2 *Dt = d.D + t * n3;
         const double2 *RttJ = Rtt + (long long)sj * n * n, *RttL = Rtt + (long long)sl * n * n;
         const double2 *QtM = Qt + (long long)mu2 * n * n, *QtN = Qt + (long long)nu2 * n * n;
 #pragma unroll 4
@@ -213,7 +216,25 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
             const double2 pi = c_mul(g22, c_sub(QtM[nu1 * n + mu1], QtN[nu1 * n + mu1]));
             const double2 piP = c_mul(Gs[nu1 * GLD + mu1], c_sub(qb[cl], qa[rl]));
             const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
-            Ks[cl * KLD + rl] = K;
+            if (fused) {
+                // RK4 bookkeeping of this element right away (off-diagonal tile pairs)
+                const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : Ac[e], c_scale(K, st.w));
+                double2 v;
+                if (k < 3) {
+                    Ac[e] = rk;
+                    v = c_add(Yc[e], c_scale(K, st.c_next));
+                } else {
+                    v = c_add(Yc[e], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
+                    Yc[e] = v;
+                }
+                Ks[cl * KLD + rl] = v;
+                if (mu2 == nu2) {
+                    Dt[((long long)mu1 * n + nu1) * n + mu2] = v;
+                    Dt[((long long)nu1 * n + mu1) * n + nu2] = c_conj(v);
+                }
+            } else {
+                Ks[cl * KLD + rl] = K;
+            }
         }
     } else {
 #pragma unroll 4
@@ -277,7 +298,7 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
     }
     // RK4 bookkeeping on the compressed state; next-stage input value in Ks
     double2 *Dt = d.D + t * n3;
-    for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+    for (int e = threadIdx.x; e < kTB * kTB && !fused; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
         const double2 K = Ks[cl * KLD + rl];
         const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : Ac[e], c_scale(K, st.w));
