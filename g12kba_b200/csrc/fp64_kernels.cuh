@@ -150,7 +150,10 @@ __device__ __forceinline__ void step_begin_body(const Dev &d)
 static __global__ void __launch_bounds__(256) k_step_begin(Dev d) { step_begin_body(d); }
 
 // HF.h:57-104, entry by entry.
-__device__ __forceinline__ double2 h_entry(const Dev &d, const double2 *G, int mu, int nu, const StageP &st)
+// gd: the diagonal G[p][p] of the stage's G1 (staged in shared memory by the
+// caller; the diagonal entries of h sum up to 4 Nv of them)
+__device__ __forceinline__ double2 h_entry(const Dev &d, const double2 *G, const double2 *gd, int mu, int nu,
+                                           const StageP &st)
 {
     const int Ns = d.Ns, n = d.n;
     const int i = mu % Ns, a = mu / Ns, j = nu % Ns, b = nu / Ns;
@@ -158,22 +161,22 @@ __device__ __forceinline__ double2 h_entry(const Dev &d, const double2 *G, int m
     double2 v = make_double2(0.0, 0.0);
     if (mu == nu) {
         if (i < st.nq) v.x += st.wq;
-        v = c_add(v, c_scale(c_mi(G[mu * n + mu]), U));
+        v = c_add(v, c_scale(c_mi(gd[mu]), U));
         for (int g = 0; g < d.Nb; ++g)
             if (g != a) {
                 int ig = i + g * Ns;
-                v = c_add(v, c_scale(c_mi(G[ig * n + ig]), 2.0 * U));
+                v = c_add(v, c_scale(c_mi(gd[ig]), 2.0 * U));
             }
         for (int m = 1; m <= d.nv; ++m) {
             const double Vm = U * d.law[m - 1];
             for (int dd = 0; dd < d.Nb; ++dd) {
                 if (i + m < Ns) {
                     int p = (i + m) + dd * Ns;
-                    v = c_add(v, c_scale(c_mi(G[p * n + p]), 2.0 * Vm));
+                    v = c_add(v, c_scale(c_mi(gd[p]), 2.0 * Vm));
                 }
                 if (i - m >= 0) {
                     int q = (i - m) + dd * Ns;
-                    v = c_add(v, c_scale(c_mi(G[q * n + q]), 2.0 * Vm));
+                    v = c_add(v, c_scale(c_mi(gd[q]), 2.0 * Vm));
                 }
             }
         }
@@ -247,10 +250,13 @@ __device__ __forceinline__ void prep_body(const Dev &d, int k, int bx)
     const double2 *__restrict__ G = g1_stage(d, k);
     const int pair_blocks = prep_pair_blocks(n2);
     if (bx >= pair_blocks) {
+        extern __shared__ double2 sm_h[];
+        for (int p = threadIdx.x; p < n; p += blockDim.x) sm_h[p] = G[(long long)p * n + p];
+        __syncthreads();
         const long long x = (long long)(bx - pair_blocks) * blockDim.x + threadIdx.x;
         double2 hv = make_double2(0.0, 0.0);
         if (x < n2) {
-            hv = h_entry(d, G, int(x / n), int(x % n), st);
+            hv = h_entry(d, G, sm_h, int(x / n), int(x % n), st);
             d.h[x] = hv;
         }
         if (d.ozb) h_digits(d, hv, int(x));
