@@ -233,7 +233,7 @@ def ensemble_measure(g12, local, rank=0, world=1, pg=None, steps=20, warmup=3, s
                     f"does not depend on the state)"}
 
 
-def learned_measure(g12, local, ntrain=64, ntest=8, T=3000, P=400, train_steps=8000, judge_every=200):
+def learned_measure(g12, local, ntrain=128, ntest=8, T=3000, P=400, train_steps=20000, judge_every=200):
     """Learned extrapolator on its n=16 family (Ns=8, Nb=2, U ~ U[1,3],
     quench ~ U[0.5,3] switched on at t=1): trajectories from the batch engine,
     training on the GPU, rollout of held-out systems from an RK4 prefix of P

@@ -213,6 +213,18 @@ void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
     k_step_begin<<<1, 256, 0, s>>>(d);
     for (int k = 0; k < 4; ++k) {
         k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, s>>>(d, k);
+        if (ctx->prec != G12_PREC_FP64 && d.gate) {
+            // symmetric engine: k_g1 forks after the GEMM (one 201 KB CTA per SM,
+            // which k_g1's blocks would keep off their SMs) and overlaps the epilogue
+            mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, 0, s);
+            cudaEventRecord(ctx->ev_fork, s);
+            cudaStreamWaitEvent(ctx->s2, ctx->ev_fork, 0);
+            k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s2>>>(d, k);
+            cudaEventRecord(ctx->ev_join, ctx->s2);
+            mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, 1, s);
+            cudaStreamWaitEvent(s, ctx->ev_join, 0);
+            continue;
+        }
         cudaEventRecord(ctx->ev_fork, s);
         cudaStreamWaitEvent(ctx->s2, ctx->ev_fork, 0);
         k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s2>>>(d, k);
