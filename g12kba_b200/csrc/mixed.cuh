@@ -27,7 +27,7 @@ struct MixedState {
     SymDev s{};
     CUtensorMap map_a{}, map_b{};  // TMA views of TMPa / TMPb
     unsigned char *ozb = nullptr;  // h digit tiles (written by k_prep, read by k_sym_gemm_oz2)
-    int oz2 = 0;  // warp-specialised digit GEMM (G12KBA_OZ_SIMPLE=1 selects the single-role kernel)
+    int oz2 = 0;  // bf16 digit GEMM (k_sym_gemm_oz2)
     size_t epi_smem = 0, simt_smem = 0, tc_smem = 0;
     int tc_grid = 0;
     std::vector<void *> allocs;
@@ -154,20 +154,13 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
         if (!encode_tmp_map(&m.map_a, s.TMPa, n, err) || !encode_tmp_map(&m.map_b, s.TMPb, n, err)) return -2;
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-        const char *ov = getenv("G12KBA_OZ_SIMPLE");
-        m.oz2 = m.oz && !(ov && ov[0] == '1');
+        m.oz2 = m.oz;
         if (m.oz2 && n == 32) {
             m.tc_smem = Oz2Shape<32>::SMEM;
             cudaFuncSetAttribute(k_sym_gemm_oz2<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.tc_smem));
         } else if (m.oz2) {
             m.tc_smem = Oz2Shape<16>::SMEM;
             cudaFuncSetAttribute(k_sym_gemm_oz2<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.tc_smem));
-        } else if (m.oz && n == 32) {
-            m.tc_smem = OzShape<32>::SMEM;
-            cudaFuncSetAttribute(k_sym_gemm_oz<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.tc_smem));
-        } else if (m.oz) {
-            m.tc_smem = OzShape<16>::SMEM;
-            cudaFuncSetAttribute(k_sym_gemm_oz<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.tc_smem));
         } else if (n == 32 && m.pieces == 2) {
             m.tc_smem = TcShape<32, 2>::SMEM;
             cudaFuncSetAttribute(k_sym_gemm_tc<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.tc_smem));
@@ -181,11 +174,11 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
             m.tc_smem = TcShape<16, 3>::SMEM;
             cudaFuncSetAttribute(k_sym_gemm_tc<16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.tc_smem));
         }
-        if (m.oz2 && !mixed_alloc(m, &m.ozb, size_t(kOzDigits) * Oz2Shape<32>::B_BYTES + 4 * 64)) {
+        if (m.oz2 && !mixed_alloc(m, &m.ozb, size_t(kOz2Digits) * Oz2Shape<32>::B_BYTES + 4 * 64)) {
             if (err) *err = "out of device memory (mixed engine)";
             return -3;
         }
-        m.tc_grid = m.oz2 ? std::min(2 * s.gemm_tiles, sms) : std::min(2 * s.gemm_tiles, 2 * sms);
+        m.tc_grid = m.oz2 ? std::min(2 * s.gemm_tiles, sms) : std::min(2 * s.gemm_tiles, 2 * sms);  // oz2: persistent
     }
     if (cudaGetLastError() != cudaSuccess) {
         if (err) *err = "mixed engine set-up failed";
@@ -222,7 +215,7 @@ inline int mixed_kernel_kinds(const MixedState &) { return 2; }
 
 inline const char *mixed_kernel_name(const MixedState &m, int q)
 {
-    if (q == 0) return m.oz2 ? "k_sym_gemm_oz2" : m.oz ? "k_sym_gemm_oz" : (m.tc ? "k_sym_gemm_tc" : "k_sym_gemm_simt");
+    if (q == 0) return m.oz2 ? "k_sym_gemm_oz2" : (m.tc ? "k_sym_gemm_tc" : "k_sym_gemm_simt");
     if (q == 1) return "k_sym_epi";
     return "";
 }
@@ -236,8 +229,6 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
             const CUtensorMap &map = (k & 1) ? m.map_a : m.map_b;
             if (m.oz2 && s.n == 32) k_sym_gemm_oz2<32><<<m.tc_grid, kOz2Threads, m.tc_smem, st>>>(s, k, map);
             else if (m.oz2) k_sym_gemm_oz2<16><<<m.tc_grid, kOz2Threads, m.tc_smem, st>>>(s, k, map);
-            else if (m.oz && s.n == 32) k_sym_gemm_oz<32><<<m.tc_grid, kOzThreads, m.tc_smem, st>>>(s, k);
-            else if (m.oz) k_sym_gemm_oz<16><<<m.tc_grid, kOzThreads, m.tc_smem, st>>>(s, k);
             else if (s.n == 32 && m.pieces == 2) k_sym_gemm_tc<32, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (s.n == 32) k_sym_gemm_tc<32, 3><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (m.pieces == 2) k_sym_gemm_tc<16, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);

@@ -1,27 +1,16 @@
-// tcgen05 (sm_100a) W contraction with exact integer-digit products
-// (error-free splitting after Ozaki, Ogita, Oishi and Rump, "Error-free
-// transformations of matrix multiplication by using fast routines of matrix
-// multiplication and its applications", Numer. Algorithms 59 (2012)).
+// tcgen05 (sm_100a) W contraction of the symmetric engine with exact
+// integer-digit products (error-free splitting after Ozaki, Ogita, Oishi and
+// Rump, "Error-free transformations of matrix multiplication by using fast
+// routines of matrix multiplication and its applications", Numer. Algorithms
+// 59 (2012)).
 //
 // Why: tcgen05 kind::tf32 / kind::f16 accumulate in FP32 with a rounding that
 // is biased toward zero (measured on B200: about -4e-8 relative per W
 // element).  A uniformly shrunk commutator acts like a rescaled Hamiltonian,
 // so the phase error of G1 grows linearly in time (1.5e-5 after the 10,000-step
-// n = 32 run).  Here every partial sum is an integer below 2^24, so the FP32
-// accumulation is exact whatever its rounding mode.
-//
-// Each A row m (and each B row j) is written as
-//   a = 2^(e_m - 6) * (d0 + d1 2^-7 + d2 2^-14 + d3 2^-21),
-// with e_m = floor(log2 max_k |a|), |d0| <= 128 and |d1..d3| <= 64 obtained by
-// successive round-to-nearest (so the truncation after d3, <= 2^-28 of the row
-// maximum, is unbiased).  The digits are held exactly in bf16.  The products
-// with digit-level i + j = L (L = 0..3) accumulate in TMEM accumulator L:
-//   |sum| <= (L+1) * K * 128 * 128 <= 4 * 64 * 2^14 = 2^22 < 2^24  (exact).
-// T1 = 2^(e_m - 6) 2^(e_j - 6) sum_L 2^(-7L) P_L is formed in FP64.
-//
-// Tile and operands as in sym_tc.cuh, except that the FP32 rows are read by the
-// threads (two rows per warp per load, coalesced) and digit-split straight into
-// 128-byte-swizzled bf16 rows; K = 2n bf16 = 128 (n = 32) or 64 (n = 16) bytes.
+// n = 32 run with TF32x3).  Here every partial sum is an integer below 2^24, so
+// the FP32 accumulation is exact whatever its rounding mode.  The digit format
+// and the kernel's roles are described at k_sym_gemm_oz2.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -32,8 +21,6 @@
 
 namespace g12 {
 
-constexpr int kOzDigits = 4;
-constexpr int kOzLevels = 4;
 
 // D f32, A/B bf16, K-major, M = 128, N = n_cols
 __host__ __device__ constexpr uint32_t umma_idesc_bf16(int n_cols)
@@ -65,25 +52,17 @@ __device__ __forceinline__ float rint_small_mul(float a, float b)
     return __fadd_rn(__fmaf_rn(a, b, 12582912.0f), -12582912.0f);
 }
 
-// digits of x (already scaled so that |x| < 2^21): x = d0 2^14 + d1 2^7 + d2 + d3 2^-7 + r,
-// every step exact except the final remainder
-__device__ __forceinline__ void oz_digits(float x, float (&d)[kOzDigits])
-{
-    float r = x;
-    d[0] = rint_small_mul(r, 1.0f / 16384.0f);
-    r = __fmaf_rn(-d[0], 16384.0f, r);
-    d[1] = rint_small_mul(r, 1.0f / 128.0f);
-    r = __fmaf_rn(-d[1], 128.0f, r);
-    d[2] = rint_small(r);
-    r = __fadd_rn(r, -d[2]);
-    d[3] = rint_small_mul(r, 128.0f);
-}
 
 // two small integers (|d| <= 256, exact in bf16) -> packed bf16x2 (a in the low
 // half): the bf16 of such a value is the upper half of its FP32 bit pattern
 __device__ __forceinline__ uint32_t bf16x2_of_ints(float a, float b)
 {
     return __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x7632);
+}
+
+__device__ __forceinline__ int swz_byte(int row, int kk2)  // bf16 element kk2 of a 128-byte swizzled row
+{
+    return row * 128 + ((((kk2 >> 3) ^ (row & 7)) << 4) | ((kk2 & 7) << 1));
 }
 
 __device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }  // |e| < 127
@@ -156,244 +135,6 @@ __device__ __forceinline__ void tmem_ldw(uint32_t taddr, float (&v)[W])
 {
     if constexpr (W == 32) tmem_ld32(taddr, v);
     else tmem_ld16(taddr, v);
-}
-
-constexpr int kOzThreads = 256;
-
-template <int NN>
-struct OzShape {
-    static constexpr int N = 2 * NN;           // UMMA N
-    static constexpr int K = 2 * NN;           // real K (bf16 elements per row)
-    static constexpr int KS = K / 16;          // 32-byte K steps per product
-    static constexpr int CPT = 128 / NN;
-    static constexpr int ROW_BYTES = 128;      // one 128-byte swizzled row (zero-padded for n = 16)
-    static constexpr int A_BYTES = 128 * ROW_BYTES;
-    static constexpr int B_BYTES = N * ROW_BYTES;
-    static constexpr int TMEM_COLS = kOzLevels * N;  // 256 (n = 32) or 128 (n = 16)
-    static constexpr int OFF_A = 0;                               // kOzDigits x A_BYTES
-    static constexpr int OFF_B = kOzDigits * A_BYTES;             // kOzDigits x B_BYTES
-    static constexpr int OFF_EA = OFF_B + kOzDigits * B_BYTES;    // 128 ints
-    static constexpr int OFF_EB = OFF_EA + 128 * 4;               // N ints, then N doubles (scales)
-    static constexpr int OFF_BAR = OFF_EB + 256 * 4 + 128 * 8;
-    static constexpr int SMEM = OFF_BAR + 64 + 1024;
-    static constexpr int S_LD = N + 1;
-    static constexpr int LPR = K * 4 / 16;    // lanes per FP32 row (16-byte loads): 16 or 8
-    static constexpr int RPW = 32 / LPR;      // rows per warp load: 2 or 4
-    static constexpr int WARPS = kOzThreads / 32;
-    static constexpr int ITER = 128 / (WARPS * RPW);  // row loads per warp per tile
-    static constexpr int HALF = N / 2;                // TMEM columns per warp (two warps per lane quadrant)
-    static_assert(128 * S_LD * 4 <= kOzDigits * A_BYTES, "staging must fit in the digit buffers");
-    static_assert(TMEM_COLS <= 256, "two CTAs per SM share 512 TMEM columns");
-};
-
-__device__ __forceinline__ int swz_byte(int row, int kk2)  // bf16 element kk2 of a 128-byte swizzled row
-{
-    return row * 128 + ((((kk2 >> 3) ^ (row & 7)) << 4) | ((kk2 & 7) << 1));
-}
-
-template <int NN>
-__global__ void __launch_bounds__(kOzThreads, 2) k_sym_gemm_oz(SymDev s, int k)
-{
-    using Sh = OzShape<NN>;
-    if (!*s.d.active) return;
-    extern __shared__ unsigned char smraw[];
-    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
-    unsigned char *Ad = sm + Sh::OFF_A;
-    unsigned char *Bd = sm + Sh::OFF_B;
-    int *eA = reinterpret_cast<int *>(sm + Sh::OFF_EA);
-    int *eB = reinterpret_cast<int *>(sm + Sh::OFF_EB);
-    uint64_t *bar_mma = reinterpret_cast<uint64_t *>(sm + Sh::OFF_BAR);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar_mma + 1);
-    float *S = reinterpret_cast<float *>(Ad);  // staging reuses the A digit buffers after the MMAs
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const long long n2 = (long long)NN * NN;
-
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(Sh::TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    if (tid == 0) {
-        mbar_init(bar_mma, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    // zero the digit buffers once (the n = 16 rows use half of each 128-byte row)
-    for (int i = tid; i < (Sh::OFF_EA) / 16; i += blockDim.x) reinterpret_cast<uint4 *>(sm)[i] = make_uint4(0, 0, 0, 0);
-    __syncthreads();
-    // B digits: rows j of the real form of h^T (FP64).  h is staged in the (not
-    // yet used) A digit area, then one thread per row finds the row maximum and
-    // all threads write digits.
-    double2 *hs = reinterpret_cast<double2 *>(Ad);
-#pragma unroll 4
-    for (int x = tid; x < NN * NN; x += blockDim.x) hs[x] = s.d.h[x];
-    __syncthreads();
-    auto bval = [&](int j, int kk) -> double {
-        const int po = j / NN, mu1 = j % NN, pi = kk / NN, rho = kk % NN;
-        const double2 hv = hs[mu1 * NN + rho];
-        return (po == 0) ? ((pi == 0) ? hv.x : -hv.y) : ((pi == 0) ? hv.y : hv.x);
-    };
-    double *sB = reinterpret_cast<double *>(sm + Sh::OFF_EB + 256 * 4);  // per-row scale 2^(e_j - 6)
-    for (int j = tid; j < Sh::N; j += blockDim.x) {
-        double mx = 0.0;
-        for (int kk = 0; kk < Sh::K; ++kk) mx = fmax(mx, fabs(bval(j, kk)));
-        const int e = (mx > 0.0) ? ilogb(mx) : 0;
-        eB[j] = e;
-        sB[j] = ldexp(1.0, e - 6);
-    }
-    __syncthreads();
-    for (int x = tid; x < Sh::N * Sh::K; x += blockDim.x) {
-        const int jj = x / Sh::K, kk = x % Sh::K;
-        double r = ldexp(bval(jj, kk), 20 - eB[jj]);
-        float d[kOzDigits];
-        d[0] = float(rint(r / 16384.0));
-        r -= double(d[0]) * 16384.0;
-        d[1] = float(rint(r / 128.0));
-        r -= double(d[1]) * 128.0;
-        d[2] = float(rint(r));
-        r -= double(d[2]);
-        d[3] = float(rint(r * 128.0));
-#pragma unroll
-        for (int q = 0; q < kOzDigits; ++q)
-            *reinterpret_cast<__nv_bfloat16 *>(Bd + q * Sh::B_BYTES + swz_byte(jj, kk)) = __float2bfloat16_rn(d[q]);
-    }
-    __syncthreads();
-    // the staged h lives in the A digit area: clear it before the first tile
-    for (int i = tid; i < kOzDigits * Sh::A_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4 *>(Ad)[i] = make_uint4(0, 0, 0, 0);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t idesc = umma_idesc_bf16(Sh::N);
-    const int ntiles = 2 * s.gemm_tiles;
-    uint32_t phase = 0;
-    bool ok = true;
-    __shared__ int tile_c[Sh::CPT], tile_p[Sh::CPT];
-    constexpr int ITER = Sh::ITER;
-    const int sub = lane / Sh::LPR, sl = lane % Sh::LPR;  // row within the warp load, lane within the row
-    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const int t = tile / s.gemm_tiles, g = tile % s.gemm_tiles;
-        if (tid < Sh::CPT) {
-            tile_c[tid] = s.gemm_c[g * Sh::CPT + tid];
-            tile_p[tid] = s.gemm_partner[g * Sh::CPT + tid];
-        }
-        __syncthreads();
-        const float *Xg = sym_in(s, k) + t * 2 * s.n4;
-        // A digits: rows m = slot*NN + mu2; all loads of the tile issued first
-        float4 v[ITER];
-#pragma unroll
-        for (int it = 0; it < ITER; ++it) {
-            const int m = (warp + Sh::WARPS * it) * Sh::RPW + sub;
-            const int slot = m / NN, mu2 = m % NN;
-            v[it] = reinterpret_cast<const float4 *>(Xg + ((long long)mu2 * n2 + tile_c[slot]) * Sh::K)[sl];
-        }
-#pragma unroll
-        for (int it = 0; it < ITER; ++it) {
-            const int m = (warp + Sh::WARPS * it) * Sh::RPW + sub;
-            float mx = fmaxf(fmaxf(fabsf(v[it].x), fabsf(v[it].y)), fmaxf(fabsf(v[it].z), fabsf(v[it].w)));
-#pragma unroll
-            for (int o = Sh::LPR / 2; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            // exponent of the row maximum straight from the bits (mx is normal or zero)
-            // (clamped: rows below 2^-100 keep 2^-128 absolute accuracy, far under the state's scale)
-            const int e = (mx > 0.f) ? max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, -100) : 0;
-            if (sl == 0) eA[m] = e;
-            const float sc = pow2f(20 - e);
-            const float vv[4] = {v[it].x * sc, v[it].y * sc, v[it].z * sc, v[it].w * sc};
-            float d[kOzDigits][4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                float dd[kOzDigits];
-                oz_digits(vv[i], dd);
-#pragma unroll
-                for (int q = 0; q < kOzDigits; ++q) d[q][i] = dd[q];
-            }
-            const int kk0 = sl * 4;
-#pragma unroll
-            for (int q = 0; q < kOzDigits; ++q) {
-                const __nv_bfloat162 lo = __floats2bfloat162_rn(d[q][0], d[q][1]);
-                const __nv_bfloat162 hi = __floats2bfloat162_rn(d[q][2], d[q][3]);
-                uint2 w;
-                w.x = *reinterpret_cast<const uint32_t *>(&lo);
-                w.y = *reinterpret_cast<const uint32_t *>(&hi);
-                *reinterpret_cast<uint2 *>(Ad + q * Sh::A_BYTES + swz_byte(m, kk0)) = w;
-            }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        if (tid == 0) {
-            const uint32_t ab = smem_u32(Ad), bb = smem_u32(Bd);
-            for (int L = 0; L < kOzLevels; ++L) {
-                uint32_t acc = 0;
-                for (int i = 0; i <= L; ++i) {
-                    const int j = L - i;
-                    for (int ks = 0; ks < Sh::KS; ++ks) {
-                        umma_bf16(tmem + L * Sh::N, umma_desc_sw128(ab + i * Sh::A_BYTES + ks * 32),
-                                  umma_desc_sw128(bb + j * Sh::B_BYTES + ks * 32), idesc, acc);
-                        acc = 1;
-                    }
-                }
-            }
-            umma_commit(bar_mma);
-        }
-        ok = mbar_wait(bar_mma, phase);
-        ok = __syncthreads_and(ok);
-        if (!ok) {
-            if (tid == 0) atomicExch(s.err, 3);
-            break;
-        }
-        tc_fence_after();
-        // TMEM -> FP64 combination -> FP32 staging S[row][j]; two warps per lane
-        // quadrant, each taking half of the columns
-        {
-            const int quad = warp & 3, half = warp >> 2;
-            const int row = quad * 32 + lane;
-            const double sa = ldexp(1.0, eA[row] - 6);
-            const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + half * Sh::HALF;
-            double acc[Sh::HALF];
-#pragma unroll
-            for (int i = 0; i < Sh::HALF; ++i) acc[i] = 0.0;
-#pragma unroll
-            for (int L = kOzLevels - 1; L >= 0; --L) {
-                float v[Sh::HALF];
-                tmem_ldw<Sh::HALF>(ta + L * Sh::N, v);
-                // sum_L 2^(-7L) P_L, smallest level first
-#pragma unroll
-                for (int i = 0; i < Sh::HALF; ++i) acc[i] = acc[i] * 0x1p-7 + double(v[i]);
-            }
-#pragma unroll
-            for (int i = 0; i < Sh::HALF; ++i) {
-                const int j = half * Sh::HALF + i;
-                S[row * Sh::S_LD + j] = float(acc[i] * sa * sB[j]);
-            }
-        }
-        tc_fence_before();
-        __syncthreads();
-        // W[mu1][mu2][c] = T1[mu1][mu2][c] + T1[mu2][mu1][cbar]; stores run along r
-        float *Wg = s.W + t * 2 * s.n4;
-#pragma unroll 1
-        for (int sp = 0; sp < Sh::CPT * 2; ++sp) {
-            const int slot = sp >> 1, part = sp & 1;
-            const int ps = tile_p[slot];
-            float *Wrow = Wg + ((long long)tile_c[slot] * 2 + part) * n2;
-#pragma unroll
-            for (int r = tid; r < NN * NN; r += kOzThreads) {
-                const int mu1 = r % NN, mu2 = r / NN;
-                Wrow[r] = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] + S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
-            }
-        }
-        // (the staging overwrote the digit buffers; the MMAs read only the K steps
-        // the next tile rewrites, so no clearing is needed)
-        __syncthreads();
-        phase ^= 1;
-    }
-    if (!ok) mbar_wait(bar_mma, phase);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Sh::TMEM_COLS) : "memory");
 }
 
 }  // namespace g12
