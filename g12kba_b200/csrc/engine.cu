@@ -239,7 +239,6 @@ void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
         }
         cudaStreamWaitEvent(s, ctx->ev_join, 0);
     }
-    if (ctx->evict_bytes) cudaMemsetAsync(ctx->evict_buf, 0, ctx->evict_bytes, s);
 }
 
 int build_graph(g12_ctx *ctx)
@@ -275,16 +274,33 @@ int run_steps(g12_ctx *ctx, long long steps, double *traj_out, double *dip_out, 
         const long long lim = base + chunk;
         CK(cudaMemcpyAsync(ctx->d.limit, &lim, sizeof(long long), cudaMemcpyHostToDevice, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
-        CK(cudaEventRecord(ctx->ev0, ctx->s));
         const int G = ctx->lc.steps_per_graph;
-        for (long long q = 0; q < chunk; q += G) CK(cudaGraphLaunch(ctx->graph, ctx->s));
-        CK(cudaEventRecord(ctx->ev1, ctx->s));
+        if (ctx->evict_bytes) {
+            // L2 eviction between timed graph launches: each launch is timed on
+            // its own and the eviction write follows its end event
+            for (long long q = 0; q < chunk; q += G) {
+                CK(cudaEventRecord(ctx->ev0, ctx->s));
+                CK(cudaGraphLaunch(ctx->graph, ctx->s));
+                CK(cudaEventRecord(ctx->ev1, ctx->s));
+                CK(cudaMemsetAsync(ctx->evict_buf, 0, ctx->evict_bytes, ctx->s));
+                CK(cudaEventSynchronize(ctx->ev1));
+                float ms = 0;
+                cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+                total_ms += ms;
+            }
+        } else {
+            CK(cudaEventRecord(ctx->ev0, ctx->s));
+            for (long long q = 0; q < chunk; q += G) CK(cudaGraphLaunch(ctx->graph, ctx->s));
+            CK(cudaEventRecord(ctx->ev1, ctx->s));
+        }
         int status = 0;
         CK(cudaMemcpyAsync(&status, ctx->d.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->s));
         CK(cudaStreamSynchronize(ctx->s));
-        float ms = 0;
-        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-        total_ms += ms;
+        if (!ctx->evict_bytes) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            total_ms += ms;
+        }
         long long got = chunk;
         if (status > 0) got = (long long)status - base;  // guard at step status-1
         if (recorded) {
@@ -641,6 +657,7 @@ extern "C" int32_t g12_set_l2_eviction(g12_ctx *ctx, int64_t bytes)
     if (ctx->evict_buf) cudaFree(ctx->evict_buf);
     ctx->evict_buf = nullptr;
     ctx->evict_bytes = 0;
+    ctx->lc.steps_per_graph = ctx->n <= 8 ? 8 : (ctx->n <= 16 ? 4 : 1);
     if (bytes == 0) return G12_OK;
     if (cudaMalloc(&ctx->evict_buf, size_t(bytes)) != cudaSuccess) {
         cudaGetLastError();
@@ -649,6 +666,7 @@ extern "C" int32_t g12_set_l2_eviction(g12_ctx *ctx, int64_t bytes)
         return G12_ERR_NOMEM;
     }
     ctx->evict_bytes = size_t(bytes);
+    ctx->lc.steps_per_graph = 1;  // evict between every step
     return G12_OK;
 }
 

@@ -156,11 +156,12 @@ int32_t g12_launches_per_step(const g12_ctx *ctx);
 int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms, int32_t *calls_per_step, int32_t cap);
 const char *g12_kernel_name(const g12_ctx *ctx, int32_t kind);
 
-/* Measurement aid: after every RK4 step (in g12_propagate*, g12_adiabatic_switch
- * and g12_kernel_times) write `bytes` bytes of a private device buffer, so that
- * every step starts with the state evicted from L2 (126 MB on B200), as it
- * would if the working set exceeded L2.  The write is extra work inside
- * the step, never skipped work.  0 (the default) switches it off.  No
+/* Measurement aid: with bytes > 0, g12_propagate* and g12_adiabatic_switch
+ * time every RK4 step on its own (CUDA events around the step's graph) and, after
+ * each step's end event, write `bytes` bytes of a private device buffer, so that
+ * every timed step starts with the state evicted from L2 (126 MB on B200) and the
+ * eviction write itself is not timed (g12_last_device_ms sums the steps);
+ * g12_kernel_times writes it between steps.  0 (the default) switches it off.  No
  * counterpart in the reference. */
 int32_t g12_set_l2_eviction(g12_ctx *ctx, int64_t bytes);
 
