@@ -60,6 +60,12 @@ struct Dev {
     StepP *cur;
 };
 
+// programmatic dependent launch: wait until the preceding kernel of the stream
+// has completed and its writes are visible (no effect without such a launch),
+// and let the next kernel of the stream start its prologue
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double2 c_mul(double2 a, double2 b)
@@ -376,7 +382,11 @@ __device__ __forceinline__ void prep_body(const Dev &d, int k, int bx)
     }
 }
 
-static __global__ void __launch_bounds__(kPrepWarps * 32) k_prep(Dev d, int k) { prep_body(d, k, blockIdx.x); }
+static __global__ void __launch_bounds__(kPrepWarps * 32) k_prep(Dev d, int k)
+{
+    grid_dep_launch();  // the symmetric engine's GEMM may start its prologue
+    prep_body(d, k, blockIdx.x);
+}
 
 // G1 side of a stage (commutators.h:28-51, G1_G2_t_step.h:24-47) and the
 // G1 RK bookkeeping (RK_solver.h:134-135, 204-208).  One output per thread,

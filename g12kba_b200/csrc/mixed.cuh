@@ -9,6 +9,7 @@
 #include <cudaTypedefs.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "fp64_kernels.cuh"
@@ -220,6 +221,24 @@ inline const char *mixed_kernel_name(const MixedState &m, int q)
     return "";
 }
 
+// launch with programmatic stream serialisation: the kernel may start while its
+// predecessor finishes and waits for it inside (griddepcontrol.wait)
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, cudaStream_t st)
 {
     m.s.d = d;
@@ -227,8 +246,8 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
     if (q == 0) {
         if (m.tc) {
             const CUtensorMap &map = (k & 1) ? m.map_a : m.map_b;
-            if (m.oz2 && s.n == 32) k_sym_gemm_oz2<32><<<m.tc_grid, kOz2Threads, m.tc_smem, st>>>(s, k, map);
-            else if (m.oz2) k_sym_gemm_oz2<16><<<m.tc_grid, kOz2Threads, m.tc_smem, st>>>(s, k, map);
+            if (m.oz2 && s.n == 32) launch_pdl(k_sym_gemm_oz2<32>, dim3(m.tc_grid), dim3(kOz2Threads), m.tc_smem, st, s, k, map);
+            else if (m.oz2) launch_pdl(k_sym_gemm_oz2<16>, dim3(m.tc_grid), dim3(kOz2Threads), m.tc_smem, st, s, k, map);
             else if (s.n == 32 && m.pieces == 2) k_sym_gemm_tc<32, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (s.n == 32) k_sym_gemm_tc<32, 3><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (m.pieces == 2) k_sym_gemm_tc<16, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
@@ -238,7 +257,9 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
         }
     } else {
         const dim3 g(s.npairs, 2);
-        if (s.n == 32) k_sym_epi<32><<<g, 256, m.epi_smem, st>>>(s, k);
+        if (s.n == 32 && m.oz2) launch_pdl(k_sym_epi<32>, g, dim3(256), m.epi_smem, st, s, k);
+        else if (s.n == 16 && m.oz2) launch_pdl(k_sym_epi<16>, g, dim3(256), m.epi_smem, st, s, k);
+        else if (s.n == 32) k_sym_epi<32><<<g, 256, m.epi_smem, st>>>(s, k);
         else if (s.n == 16) k_sym_epi<16><<<g, 256, m.epi_smem, st>>>(s, k);
         else if (s.n == 8) k_sym_epi<8><<<g, 256, m.epi_smem, st>>>(s, k);
         else k_sym_epi<64><<<g, 256, m.epi_smem, st>>>(s, k);

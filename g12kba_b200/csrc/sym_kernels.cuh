@@ -135,6 +135,9 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
     if (threadIdx.x < NN) site[threadIdx.x] = threadIdx.x % Ns;
 #pragma unroll 4
     for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[(x / n) * GLD + x % n] = G1[x];
+    // W comes from the GEMM launched just before this kernel (G1 and the tables
+    // of k_prep were complete before it started)
+    grid_dep_wait();
 #pragma unroll
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;

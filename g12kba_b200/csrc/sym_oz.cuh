@@ -270,6 +270,10 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
+    // everything above is independent of the preceding kernels (k_prep writes the
+    // digits of h, the previous epilogue the FP32 input)
+    grid_dep_wait();
+    grid_dep_launch();
     const uint32_t tmem = *tmem_slot;
     auto tile_c = [&](int i, int g, int slot) { return i < kOz2ListTiles ? lc[i * Sh::CPT + slot] : s.gemm_c[g * Sh::CPT + slot]; };
     auto tile_p = [&](int i, int g, int slot) {
