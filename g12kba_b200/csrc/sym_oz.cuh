@@ -238,7 +238,8 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Sh::OFF_BAR);
     uint64_t *full_a = bar, *empty_a = bar + 2, *dig_full = bar + 4, *dig_empty = bar + 6, *acc_full = bar + 8,
              *acc_empty = bar + 10;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 12);
+    uint64_t *b_ready = bar + 12;  // the digits of h are in shared memory
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 13);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long n2 = (long long)NN * NN;
     const int ntiles = 2 * s.gemm_tiles;
@@ -259,6 +260,7 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
             mbar_init(&acc_full[q], 1);
             mbar_init(&acc_empty[q], 256);
         }
+        mbar_init(b_ready, 256);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // c values and partner slots of this CTA's first tiles (independent loads)
@@ -270,9 +272,12 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    // everything above is independent of the preceding kernels (k_prep writes the
-    // digits of h, the previous epilogue the FP32 input)
-    grid_dep_wait();
+    // Launched with programmatic dependence on k_prep: the FP32 input (written by
+    // the previous epilogue, which finished before k_prep started) can be loaded
+    // and digit-split at once; only the epilogue warps wait for k_prep before they
+    // copy the digits of h, and the MMA thread waits for that copy.  The next
+    // kernel (the epilogue) waits for this whole grid, which cannot finish before
+    // k_prep has, so it may be scheduled right away.
     grid_dep_launch();
     const uint32_t tmem = *tmem_slot;
     auto tile_c = [&](int i, int g, int slot) { return i < kOz2ListTiles ? lc[i * Sh::CPT + slot] : s.gemm_c[g * Sh::CPT + slot]; };
@@ -308,27 +313,17 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
             }
         }
     } else {
-        // warps 1-17: digit buffers start at zero (the n = 16 rows fill half of
-        // each 128-byte row); B digit tiles and row scales of h from k_prep
-        for (int i = tid - 32; i < Sh::DSETS * Sh::D_SET / 16; i += blockDim.x - 32)
-            reinterpret_cast<uint4 *>(Ds)[i] = make_uint4(0, 0, 0, 0);
-        const uint4 *bsrc = reinterpret_cast<const uint4 *>(s.d.ozb);
-        for (int i = tid - 32; i < kOz2Digits * Sh::B_BYTES / 16; i += blockDim.x - 32)
-            reinterpret_cast<uint4 *>(Bd)[i] = bsrc[i];
-        const float *sbsrc = reinterpret_cast<const float *>(s.d.ozb + kOz2Digits * Sh::B_BYTES);
-        for (int j = tid - 32; j < Sh::N; j += blockDim.x - 32) sB[j] = sbsrc[j];
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc_fence_before();
-        named_sync(2, kOz2Threads - 32);
-        tc_fence_after();
-
         if (warp == 1) {
             // ---- MMA issuer
             if (lane == 0) {
+                if (!mbar_wait(b_ready, 0)) {
+                    ok = false;
+                    atomicExch(s.err, 8);
+                }
                 const uint32_t idesc = umma_idesc_bf16(Sh::N);
                 const uint32_t bb = smem_u32(Bd);
                 int done = 0;
-                for (int i = 0; i < my_tiles; ++i) {
+                for (int i = 0; i < my_tiles && ok; ++i) {
                     const int b = i & 1, db = i % Sh::DSETS, du = i / Sh::DSETS;
                     if (!mbar_wait(&dig_full[db], du & 1) ||
                         (i >= 2 && !mbar_wait(&acc_empty[b], ((i - 2) >> 1) & 1))) {
@@ -361,6 +356,10 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
             }
         } else if (warp < 10) {
             // ---- digit split: threads (2m, 2m+1) share row m, each half of its K values
+            // the digit buffers start at zero (the n = 16 rows fill half of each
+            // 128-byte row; the fence before each dig_full arrival covers them)
+            for (int i = tid - 64; i < Sh::DSETS * Sh::D_SET / 16; i += 256)
+                reinterpret_cast<uint4 *>(Ds)[i] = make_uint4(0, 0, 0, 0);
             const int dt = tid - 64;
             const int m = dt >> 1, half = dt & 1;
             const int sw = m & 7;
@@ -419,6 +418,17 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
         } else {
             // ---- epilogue: warp (quadrant q, part h) reads TMEM lanes 32q..32q+31,
             // columns h*NN .. h*NN+NN-1 of every level
+            // the digits of h and their row scales, written by k_prep
+            grid_dep_wait();
+            {
+                const uint4 *bsrc = reinterpret_cast<const uint4 *>(s.d.ozb);
+                for (int i = tid - 320; i < kOz2Digits * Sh::B_BYTES / 16; i += 256)
+                    reinterpret_cast<uint4 *>(Bd)[i] = bsrc[i];
+                const float *sbsrc = reinterpret_cast<const float *>(s.d.ozb + kOz2Digits * Sh::B_BYTES);
+                for (int j = tid - 320; j < Sh::N; j += 256) sB[j] = sbsrc[j];
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                mbar_arrive(b_ready);
+            }
             const int quad = warp & 3, hp = (warp - 10) >> 2;
             const int row = quad * 32 + lane;
             const int et = tid - 320;  // 0..255
