@@ -234,11 +234,11 @@ def ensemble_measure(g12, local, rank=0, world=1, pg=None, steps=20, warmup=3, s
                     f"does not depend on the state)"}
 
 
-def learned_measure(g12, local, ntrain=128, ntest=8, T=3000, P=400, train_steps=20000, judge_every=200):
+def learned_measure(g12, local, ntrain=128, ntest=8, T=3000, P=400, train_steps=20000, check_every=200):
     """Learned extrapolator on its n=16 family (Ns=8, Nb=2, U ~ U[1,3],
     quench ~ U[0.5,3] switched on at t=1): trajectories from the batch engine,
     training on the GPU, rollout of held-out systems from an RK4 prefix of P
-    steps, judged against their RK4 trajectories every `judge_every` steps."""
+    steps, checked against their RK4 trajectories every `check_every` steps."""
     import torch
     from g12kba_b200 import learned as L
     ps = L.window_params(ntrain + ntest, seed=5, time_steps=T)
@@ -261,7 +261,7 @@ def learned_measure(g12, local, ntrain=128, ntest=8, T=3000, P=400, train_steps=
     pred = pred.cpu().numpy()
     errs = L.running_errors(pred, truth, 16, P - 1)
     h3, h2 = L.horizon(errs, 1e-3), L.horizon(errs, 1e-2)
-    cks, ce = L.checkpoint_errors(pred, truth, 16, P - 1, judge_every)
+    cks, ce = L.checkpoint_errors(pred, truth, 16, P - 1, check_every)
     # plain RK4 on one of these systems (FP64 and the mixed engine)
     rk = {}
     for prec in ("fp64", "bf16oz"):
@@ -293,13 +293,13 @@ def learned_measure(g12, local, ntrain=128, ntest=8, T=3000, P=400, train_steps=
                             "device_ms": net_ms, "trajectories": int(fte.shape[0])},
         "plain_rk4_simulated_time_per_s": {k: dt * v for k, v in rk.items()},
         "horizon_steps_median_err_le_1e-3": h3, "horizon_steps_median_err_le_1e-2": h2,
-        "judge_every_steps": judge_every,
+        "check_every_steps": check_every,
         "dmd_comparator": {"horizon_steps_median_err_le_1e-3": L.horizon(derr, 1e-3),
                            "horizon_steps_median_err_le_1e-2": L.horizon(derr, 1e-2),
                            "median_err_after_200_steps": float(np.median(derr[:, min(199, derr.shape[1] - 1)])),
                            "host_seconds": dmd_s, "window": min(P - 1, 400)},
         "network_median_err_after_200_steps": float(np.median(errs[:, min(199, errs.shape[1] - 1)])),
-        "judge_checkpoint_median_err": {int(c): float(np.median(ce[:, i])) for i, c in enumerate(cks[:10])},
+        "checkpoint_median_err": {int(c): float(np.median(ce[:, i])) for i, c in enumerate(cks[:10])},
         "simulated_time_per_s_within_1e-3": covered(h3),
         "speedup_vs_plain_fp64_within_1e-3": covered(h3) / (dt * rk["fp64"]),
         "speedup_vs_plain_fp64_within_1e-2": covered(h2) / (dt * rk["fp64"]),

@@ -1,7 +1,7 @@
 """Learned G1 extrapolator: a network trained on trajectories that the
 propagation engine generates, mapping a window of K past G1 snapshots to the
 next M snapshots.  No counterpart in the reference (G12KBA-GW has no learned
-component); the RK4 propagation stays the judge of its error and the fallback.
+component); the RK4 propagation stays the check of its error and the fallback.
 
 Training, inference and data generation all run on the GPU through the C ABI
 (``g12_mlp_*``, ``g12_batch_propagate_features``); torch only provides device
@@ -292,7 +292,7 @@ def naive_rollout(prefix, total):
 
 
 def checkpoint_errors(pred, truth, n, t0, every):
-    """Dipole error of a rollout against the RK4 trajectory at the judge's
+    """Dipole error of a rollout against the RK4 trajectory at the RK4
     checkpoints: for each checkpoint c (every `every` snapshots after t0),
     max over snapshots t0 < s <= c of |p - p_ref| / max|p_ref| (per trajectory).
     Returns (checkpoints, errors [ntraj][ncheck])."""

@@ -25,7 +25,7 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 SHAPES = [(1, 2), (2, 1), (3, 1), (2, 2), (3, 2), (2, 3), (4, 2), (5, 1)]
 
 RUNS = {
-    # config-1 shape, shortened (BASELINE configs[0] with 200 of 2000 steps)
+    # the Ns=4, Nb=1 chain (U=1, t1=1, dt=0.02), shortened to 200 of its 2000 steps
     "run_c1_short": Config(Ns=4, Nb=1, Nq=2, time_steps=200, U=1.0, t1=1.0, t2=0.0, dt=0.02,
                            AS_rate=0.5, AS_midpoint=10, q_type="full", quench_strength=1.0),
     # extended model, Nb = 2, U/(1+r) law, pulse quench (masked by the t < 50 gate)

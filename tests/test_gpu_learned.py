@@ -1,7 +1,7 @@
 """The learned extrapolator end to end on a small family: trajectories from the
 batch engine, training on the GPU, rollout from an RK4 prefix, and what the
 trained network gains over the method without it (holding the last RK4
-snapshot) and over the untrained network, judged against the RK4 trajectory."""
+snapshot) and over the untrained network, checked against the RK4 trajectory."""
 import numpy as np
 import pytest
 

@@ -59,7 +59,7 @@ def _run(g12, p, prec, G0, nsteps):
 
 @pytest.mark.parametrize("prec", ["fp32", "bf16oz"])
 def test_mixed_propagation_vs_fp64_n16(g12, prec):
-    # configs[1] shape, adiabatic switching shortened so the run stays brief
+    # the extended model (Ns=8, Nb=2, pulse quench), adiabatic switching shortened so the run stays brief
     cfg = Config(Ns=8, Nb=2, Nq=3, time_steps=300, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, vlaw="inv",
                  q_type="pulse", quench_strength=2.0, quench_rate=2, quench_on_midpoint=15,
                  quench_off_midpoint=25, AS_rate=0.3, AS_midpoint=2.0)

@@ -148,7 +148,7 @@ def test_deterministic(g12):
 
 
 def test_n16_steps_vs_oracle(g12, oracle):
-    # configs[1] shape (Ns=8, Nb=2, EHM, U/(1+r), pulse) from a correlated state
+    # the extended model (Ns=8, Nb=2, EHM, U/(1+r), pulse quench) from a correlated state
     cfg = Config(Ns=8, Nb=2, Nq=3, time_steps=6, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, vlaw="inv",
                  q_type="pulse", quench_strength=2.0, quench_rate=2, quench_on_midpoint=15, quench_off_midpoint=25)
     p = params_of(g12, cfg)
@@ -174,7 +174,7 @@ def test_n16_steps_vs_oracle(g12, oracle):
 
 
 def test_n32_rhs_vs_oracle(g12, oracle):
-    # configs[2] size (Ns=16, Nb=2): one full right-hand side against the oracle
+    # the n=32 system (Ns=16, Nb=2): one full right-hand side against the oracle
     cfg = Config(Ns=16, Nb=2, Nq=4, U=1.5, t2=0.3, EHM=True, vlaw="inv")
     rng = np.random.default_rng(11)
     n = cfg.n
