@@ -151,7 +151,7 @@ __device__ __forceinline__ void named_sync(int id, int nthreads)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Warp-specialised, persistent digit GEMM (same tiles as k_sym_gemm_oz) with
+// Warp-specialised, persistent digit GEMM (same tiles as k_sym_gemm_tc) with
 // four 8-bit digits per operand:
 //   a = 2^(e - 6) (d0 + d1 2^-8 + d2 2^-16 + d3 2^-24),  |d_i| <= 128 (exact in bf16),
 // obtained by successive round-to-nearest of a 2^(30 - e) (e = exponent of the

@@ -47,7 +47,7 @@ enum g12_precision {
     G12_PREC_FP32 = 3,    /* symmetric engine with an FP32 CUDA-core contraction (checker) */
     G12_PREC_TF32X6 = 4   /* tcgen05 kind::tf32: 3 tf32 pieces per operand, 6 products */
 };
-/* The mixed modes (TF32X3, TF32X6, FP32) use the symmetric engine: they
+/* The mixed modes (BF16OZ, TF32X3, TF32X6, FP32) use the symmetric engine: they
  * require the physical G2 symmetries G2[mu2 mu1; nu2 nu1] = G2[mu1 mu2; nu1 nu2]
  * and G2[nu1 nu2; mu1 mu2] = conj(G2[mu1 mu2; nu1 nu2]) (every state reached
  * from G2 = 0 has them; set_state keeps the upper 32 x 32 blocks of G2 seen as
