@@ -234,6 +234,48 @@ def ensemble_measure(g12, local, rank=0, world=1, pg=None, steps=20, warmup=3, s
                     f"does not depend on the state)"}
 
 
+def extended_model_measure(g12, local):
+    """The extended model (Ns=8, Nb=2, n=16: t2=0.5, U=2, EHM w(r)=U/(1+r), pulse
+    quench 2.0 on Nq=3 with rate 2 and on/off midpoints 15/25, dt=0.01, 5000 steps
+    = 5001 iterations) in FP64 and the mixed modes, each from G0 through the
+    adiabatic switching; errors against the FP64 run.  The pulse is switched on
+    with quench_gate 0 (the reference's t<50 gate would keep it off for the whole
+    run)."""
+    p = g12.make_params(Ns=8, Nb=2, Nq=3, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, v_law="inv",
+                        q_type="pulse", quench_strength=2.0, quench_rate=2.0, quench_on_midpoint=15.0,
+                        quench_off_midpoint=25.0, time_steps=5000, quench_gate=0.0)
+    T = g12.rk_iterations(p)
+    out, ref, ref_p = {}, None, None
+    for prec in ("fp64", "bf16oz", "tf32x3"):
+        with g12.Context(p, prec, local) as ctx:
+            ctx.set_state(g12.make_G0(p))
+            ctx.adiabatic_switch()
+            traj, rc = ctx.propagate(T)
+            ms = ctx.last_device_ms
+        dip = g12.dipole(traj)
+        row = {"steps_per_s": T / (ms / 1e3), "status": rc, "iterations": T}
+        if ref is None:
+            ref, ref_p = traj, dip
+        else:
+            row["g1_max_rel_err_vs_fp64"] = float(np.max(np.abs(traj - ref)) / np.max(np.abs(ref)))
+            row["dipole_err_vs_fp64"] = float(np.max(np.abs(dip - ref_p)) / max(np.max(np.abs(ref_p)), 1e-12))
+        out[prec] = row
+    # the model's own sensitivity: plain FP64 from the same post-switching state
+    # with G1 perturbed by 1e-12 of its largest entry
+    with g12.Context(p, "fp64", local) as ctx:
+        ctx.set_state(g12.make_G0(p))
+        ctx.adiabatic_switch()
+        G1, XX, XY = ctx.get_state()
+        rng = np.random.default_rng(0)
+        dG = 1e-12 * np.abs(G1).max() * (rng.standard_normal(G1.shape) + 1j * rng.standard_normal(G1.shape))
+        ctx.set_state(G1 + (dG - np.conj(dG.T)) / 2, XX, XY)
+        traj, _ = ctx.propagate(T)
+    out["fp64_perturbed_1e-12"] = {"g1_max_rel_err_vs_fp64": float(np.max(np.abs(traj - ref)) / np.max(np.abs(ref))),
+                                   "note": "same FP64 engine, G1 perturbed by 1e-12 after the switching: the "
+                                           "growth of any small difference in this model"}
+    return out
+
+
 def learned_measure(g12, local, ntrain=128, ntest=8, T=3000, P=400, train_steps=20000, check_every=200):
     """Learned extrapolator on its n=16 family (Ns=8, Nb=2, U ~ U[1,3],
     quench ~ U[0.5,3] switched on at t=1): trajectories from the batch engine,
@@ -321,6 +363,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--no-extended", action="store_true")
     ap.add_argument("--skip-as", action="store_true",
                     help="start the timed steps from G0 (profiling runs); the cost of a step does not depend on the state")
     args = ap.parse_args()
@@ -428,6 +471,10 @@ def main():
     if not args.no_ensemble:
         ensemble = ensemble_measure(g12, local, rank, world, pg)
 
+    extended = None
+    if rank == 0 and not args.no_extended:
+        extended = extended_model_measure(g12, local)
+
     learned = None
     if rank == 0 and not args.no_learned:
         learned = learned_measure(g12, local)
@@ -453,7 +500,7 @@ def main():
             "speedup_vs_plain_fp64": value / value_fp,
             "g1_max_rel_err_vs_fp64": g1_err,
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline,
-            "kernels": kernels, "ensemble": ensemble, "learned": learned, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "kernels": kernels, "ensemble": ensemble, "extended_model_n16": extended, "learned": learned, "cpu_baseline": cpu, "clocks": clk.summary(),
         }
         print(json.dumps(line))
     if pg is not None:
