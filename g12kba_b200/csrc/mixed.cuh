@@ -246,8 +246,10 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
     if (q == 0) {
         if (m.tc) {
             const CUtensorMap &map = (k & 1) ? m.map_a : m.map_b;
-            if (m.oz2 && s.n == 32) launch_pdl(k_sym_gemm_oz2<32>, dim3(m.tc_grid), dim3(kOz2Threads), m.tc_smem, st, s, k, map);
-            else if (m.oz2) launch_pdl(k_sym_gemm_oz2<16>, dim3(m.tc_grid), dim3(kOz2Threads), m.tc_smem, st, s, k, map);
+            if (m.oz2 && s.n == 32)
+                launch_pdl(k_sym_gemm_oz2<32>, dim3(m.tc_grid), dim3(Oz2Shape<32>::THREADS), m.tc_smem, st, s, k, map);
+            else if (m.oz2)
+                launch_pdl(k_sym_gemm_oz2<16>, dim3(m.tc_grid), dim3(Oz2Shape<16>::THREADS), m.tc_smem, st, s, k, map);
             else if (s.n == 32 && m.pieces == 2) k_sym_gemm_tc<32, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (s.n == 32) k_sym_gemm_tc<32, 3><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (m.pieces == 2) k_sym_gemm_tc<16, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);

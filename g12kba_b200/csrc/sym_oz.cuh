@@ -161,20 +161,19 @@ __device__ __forceinline__ void named_sync(int id, int nthreads)
 // Products with digit levels i + j = L <= 3 accumulate in TMEM accumulator L:
 // |sum| <= 4 * K * 128 * 128 <= 2^22 < 2^24, exact in FP32 whatever the
 // accumulator's rounding; T1 = 2^(e_m - 6) 2^(e_j - 6) sum_L 2^(-8L) P_L.
-// Roles (18 warps):
+// Roles (26 warps at n = 32, 18 at n = 16):
 //   warp 0      TMA producer: FP32 A tiles into a 2-stage ring (starts as soon
 //               as the barriers exist)
 //   warp 1      one thread issues the 10 digit products per tile into one of
 //               two TMEM accumulator sets
 //   warps 2-9   digit split, two threads per A row (row max, exponent, 4 bf16
 //               digit rows)
-//   warps 10-17 epilogue, one per TMEM lane quadrant and part (real or
-//               imaginary half of the columns): TMEM -> FP32 combination ->
+//   warps 10-  epilogue (16 warps at n = 32, 8 at n = 16), four per column
+//               group, one per TMEM lane quadrant: TMEM -> FP32 combination ->
 //               staging -> W = T1 + e(T1)
 // so the loads of tile i+2, the digits and products of tile i+1 and the
 // epilogue of tile i overlap.  The digits of h come from k_prep
 // (h_digits).  Every wait is bounded.
-constexpr int kOz2Threads = 576;
 constexpr int kOz2Digits = 4;     // digits per operand = accumulation levels
 constexpr int kOz2ListTiles = 8;  // tiles per CTA whose c / partner lists are staged in shared memory
 
@@ -199,6 +198,10 @@ struct Oz2Shape {
     static constexpr int DC = KF / 8;           // 16-byte digit chunks per row (of 8 in a 128-byte row)
     static constexpr int KS = KF / 16;          // 32-byte K steps per product
     static constexpr int CPT = 128 / NN;
+    static constexpr int EPI_WARPS = (NN == 32) ? 16 : 8;  // epilogue warps
+    static constexpr int EPI = 32 * EPI_WARPS;              // epilogue threads
+    static constexpr int THREADS = 64 + 256 + EPI;
+    static constexpr int CW = N / (EPI_WARPS / 4);           // TMEM columns per epilogue warp
     static constexpr int A_STAGE = KB * 128 * 128;   // one FP32 tile
     static constexpr int D_BYTES = 128 * 128;        // one digit tile (128 rows x 128 B)
     static constexpr int D_SET = kOz2Digits * D_BYTES;
@@ -221,7 +224,7 @@ struct Oz2Shape {
 };
 
 template <int NN>
-__global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k, const __grid_constant__ CUtensorMap tmap)
+__global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDev s, int k, const __grid_constant__ CUtensorMap tmap)
 {
     using Sh = Oz2Shape<NN>;
     if (!*s.d.active) return;
@@ -258,9 +261,9 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
             mbar_init(&dig_full[q], 256);
             mbar_init(&dig_empty[q], 1);
             mbar_init(&acc_full[q], 1);
-            mbar_init(&acc_empty[q], 256);
+            mbar_init(&acc_empty[q], Sh::EPI);
         }
-        mbar_init(b_ready, 256);
+        mbar_init(b_ready, Sh::EPI);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // c values and partner slots of this CTA's first tiles (independent loads)
@@ -420,49 +423,52 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
             // columns h*NN .. h*NN+NN-1 of every level
             // the digits of h and their row scales, written by k_prep
             grid_dep_wait();
+            const int et = tid - 320;  // 0 .. EPI-1
             {
                 const uint4 *bsrc = reinterpret_cast<const uint4 *>(s.d.ozb);
-                for (int i = tid - 320; i < kOz2Digits * Sh::B_BYTES / 16; i += 256)
+                for (int i = et; i < kOz2Digits * Sh::B_BYTES / 16; i += Sh::EPI)
                     reinterpret_cast<uint4 *>(Bd)[i] = bsrc[i];
                 const float *sbsrc = reinterpret_cast<const float *>(s.d.ozb + kOz2Digits * Sh::B_BYTES);
-                for (int j = tid - 320; j < Sh::N; j += 256) sB[j] = sbsrc[j];
+                for (int j = et; j < Sh::N; j += Sh::EPI) sB[j] = sbsrc[j];
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_arrive(b_ready);
             }
-            const int quad = warp & 3, hp = (warp - 10) >> 2;
+            // warp (quadrant q, column group cg) reads TMEM lanes 32q..32q+31,
+            // columns cg*CW .. cg*CW+CW-1 of every level
+            const int ew = warp - 10;
+            const int quad = warp & 3, col0 = (ew >> 2) * Sh::CW;
             const int row = quad * 32 + lane;
-            const int et = tid - 320;  // 0..255
-            __shared__ int vote[8];
-            constexpr int LB = (NN == 32) ? 2 : kOz2Digits;  // levels per TMEM load batch (registers)
+            __shared__ int vote[Sh::EPI_WARPS];
+            constexpr int LB = 2;  // levels per TMEM load batch (registers)
             for (int i = 0; i < my_tiles; ++i) {
                 const int b = i & 1;
                 const int tile = blockIdx.x + i * gridDim.x;
                 const int t = tile / s.gemm_tiles, g = tile % s.gemm_tiles;
-                // the eight epilogue warps leave together (they share a named barrier)
+                // the epilogue warps leave together (they share a named barrier)
                 const bool w = __all_sync(0xffffffffu, mbar_wait(&acc_full[b], (i >> 1) & 1));
-                if (lane == 0) vote[warp - 10] = w ? 1 : 0;
-                named_sync(1, 256);
+                if (lane == 0) vote[ew] = w ? 1 : 0;
+                named_sync(1, Sh::EPI);
                 bool all = true;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) all = all && vote[q];
+                for (int q = 0; q < Sh::EPI_WARPS; ++q) all = all && vote[q];
                 if (!all) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
                 const float sa = pow2f(eA[(i & 3) * 128 + row] - 6);
-                const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * Sh::ACC + hp * NN;
-                float acc[NN];
+                const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * Sh::ACC + col0;
+                float acc[Sh::CW];
 #pragma unroll
-                for (int x = 0; x < NN; ++x) acc[x] = 0.f;
+                for (int x = 0; x < Sh::CW; ++x) acc[x] = 0.f;
                 // sum_L 2^(-8L) P_L, smallest level first (FP32, round to nearest);
-                // up to LB levels loaded per wait
+                // LB levels loaded per wait
 #pragma unroll
                 for (int L0 = kOz2Digits - 1; L0 >= 0; L0 -= LB) {
-                    float wv[LB][NN];
+                    float wv[LB][Sh::CW];
 #pragma unroll
                     for (int l = 0; l < LB; ++l)
-                        if (L0 - l >= 0) tmem_ldw_nowait<NN>(ta + (L0 - l) * Sh::N, wv[l]);
+                        if (L0 - l >= 0) tmem_ldw_nowait<Sh::CW>(ta + (L0 - l) * Sh::N, wv[l]);
 #pragma unroll
                     for (int l = 0; l < LB; ++l)
                         if (L0 - l >= 0) tmem_wait_ld(wv[l]);
@@ -470,14 +476,14 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
                     for (int l = 0; l < LB; ++l)
                         if (L0 - l >= 0) {
 #pragma unroll
-                            for (int x = 0; x < NN; ++x) acc[x] = fmaf(acc[x], 0x1p-8f, wv[l][x]);
+                            for (int x = 0; x < Sh::CW; ++x) acc[x] = fmaf(acc[x], 0x1p-8f, wv[l][x]);
                         }
                 }
 #pragma unroll
-                for (int x = 0; x < NN; ++x) S[row * Sh::S_LD + hp * NN + x] = acc[x] * sa * sB[hp * NN + x];
+                for (int x = 0; x < Sh::CW; ++x) S[row * Sh::S_LD + col0 + x] = acc[x] * sa * sB[col0 + x];
                 tc_fence_before();
                 mbar_arrive(&acc_empty[b]);
-                named_sync(1, 256);
+                named_sync(1, Sh::EPI);
                 float *Wg = s.W + t * 2 * s.n4;
 #pragma unroll 2
                 for (int sp = 0; sp < Sh::CPT * 2; ++sp) {
@@ -485,13 +491,13 @@ __global__ void __launch_bounds__(kOz2Threads, 1) k_sym_gemm_oz2(SymDev s, int k
                     const int ps = tile_p(i, g, slot);
                     float *Wrow = Wg + ((long long)tile_c(i, g, slot) * 2 + part) * n2;
 #pragma unroll
-                    for (int r = et; r < NN * NN; r += 256) {
+                    for (int r = et; r < NN * NN; r += Sh::EPI) {
                         const int mu1 = r % NN, mu2 = r / NN;
                         Wrow[r] = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] +
                                   S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
                     }
                 }
-                named_sync(1, 256);
+                named_sync(1, Sh::EPI);
             }
             if (!ok) atomicExch(s.err, 7);
         }
