@@ -399,13 +399,16 @@ def main():
         c.set_l2_eviction(EVICT_BYTES)
     barrier(pg)
     fp.set_state(*S)
+    E_start = fp.total_energy()
     traj_fp, rc_fp = fp.propagate(K)
     ms_fp = allmax(pg, fp.last_device_ms)
+    E_fp = fp.total_energy()
     barrier(pg)
     mx.set_state(*S)
     with Clocks(local) as clk:
         traj_mx, rc = mx.propagate(K)
         dev_ms = mx.last_device_ms
+    E_mx = mx.total_energy()
     barrier(pg)
     ms = allmax(pg, dev_ms)
     # the same steps without the eviction write (state L2-resident between steps)
@@ -499,6 +502,11 @@ def main():
                                          "status": rc_fp},
             "speedup_vs_plain_fp64": value / value_fp,
             "g1_max_rel_err_vs_fp64": g1_err,
+            "energy": {"start": float(E_start[0]), "correlation_start": float(E_start[3]),
+                       "fp64_rel_drift": float(abs(E_fp[0] - E_start[0]) / abs(E_start[0])),
+                       "mixed_rel_drift": float(abs(E_mx[0] - E_start[0]) / abs(E_start[0])),
+                       "correlation_change": float(E_mx[3] - E_start[3]),
+                       "note": "g12_total_energy before and after the timed steps (constant U, quench masked)"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline,
             "kernels": kernels, "ensemble": ensemble, "extended_model_n16": extended, "learned": learned, "cpu_baseline": cpu, "clocks": clk.summary(),
         }

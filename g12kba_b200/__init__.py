@@ -98,6 +98,7 @@ def lib():
                               _dp, _dp, _dp, _dp, _dp, _dp]
         L.g12_last_device_ms.restype = C.c_double
         L.g12_last_device_ms.argtypes = [C.c_void_p]
+        L.g12_total_energy.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int32, _dp]
         L.g12_launches_per_step.restype = C.c_int32
         L.g12_launches_per_step.argtypes = [C.c_void_p]
         L.g12_kernel_times.restype = C.c_int32
@@ -296,6 +297,15 @@ class Context:
         done = C.c_int64()
         rc = _check(lib().g12_propagate_dipole(self.h, nsteps, _ptr(p), C.byref(done)), self.h)
         return p[: done.value], rc
+
+    def total_energy(self, U_eff=None, w_quench=0.0, Nq_eff=0):
+        """Total energy of the current state (``g12_total_energy``):
+        array [E, 2 Tr[h0 rho], Tr[(h - h0) rho], correlation part].
+        U_eff defaults to the parameters' U (the value after adiabatic switching)."""
+        out = np.zeros(4)
+        U = self.p.U if U_eff is None else U_eff
+        _check(lib().g12_total_energy(self.h, float(U), float(w_quench), int(Nq_eff), _ptr(out)), self.h)
+        return out
 
     def rhs(self, G1, G2xx, G2xy, U_eff, w_quench=0.0, Nq_eff=0):
         """One RHS evaluation: dict of h, comm1, Ix, K1, K2xx, K2xy (replaces the state)."""

@@ -56,6 +56,7 @@ struct g12_ctx {
     std::vector<void *> allocs;
     void *evict_buf = nullptr;      // g12_set_l2_eviction: written after every step
     size_t evict_bytes = 0;
+    double *energy_dev = nullptr;   // g12_total_energy result (4 doubles)
 };
 
 namespace {
@@ -405,7 +406,8 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
               dalloc(ctx, &d.RK2, 2 * n4) && dalloc(ctx, &d.TMP0, 2 * n4) && dalloc(ctx, &d.TMP1, 2 * n4) &&
               dalloc(ctx, &d.TAB, 2 * n4) && dalloc(ctx, &d.D, 2 * n3) && dalloc(ctx, &d.Q, 2 * n3) &&
               dalloc(ctx, &d.Rt, n2 * p->Ns) && dalloc(ctx, &d.counter, 1) && dalloc(ctx, &d.limit, 1) &&
-              dalloc(ctx, &d.status, 1) && dalloc(ctx, &d.active, 1) && dalloc(ctx, &d.cur, 1);
+              dalloc(ctx, &d.status, 1) && dalloc(ctx, &d.active, 1) && dalloc(ctx, &d.cur, 1) &&
+              dalloc(ctx, &ctx->energy_dev, 4);
     if (!ok) return fail(G12_ERR_NOMEM);
     // trajectory ring: up to 4096 snapshots or 1 GiB
     ctx->traj_cap = std::max<long long>(1, std::min<long long>(4096, (1LL << 30) / (n2 * 16)));
@@ -641,6 +643,22 @@ extern "C" int g12_rhs(g12_ctx *ctx, const double *G1, const double *G2xx, const
         return G12_ERR_CUDA;
     }
     return rc;
+}
+
+extern "C" int g12_total_energy(g12_ctx *ctx, double U_eff, double w_quench, int32_t Nq_eff, double *E_out)
+{
+    if (!ctx || !E_out || Nq_eff < 0) return G12_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    StageP st{};
+    st.U = U_eff;
+    st.wq = w_quench;
+    st.nq = Nq_eff;
+    // Y1 and D (the particle-2 diagonal of G2) hold the current state on both engines
+    k_energy<<<1, kEnergyThreads, 0, ctx->s>>>(ctx->d, st, ctx->energy_dev);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(E_out, ctx->energy_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->s));
+    CK(cudaStreamSynchronize(ctx->s));
+    return G12_OK;
 }
 
 extern "C" double g12_last_device_ms(const g12_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }

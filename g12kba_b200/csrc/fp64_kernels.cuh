@@ -636,6 +636,63 @@ static __global__ void k_init_D(Dev d)
     }
 }
 
+// Total energy of the current state.  The reference computes none; this is
+// the energy that the G1-G2 equations conserve while h0 and U are constant:
+//   E1 = 2 Tr[h0 rho] + Tr[(h - h0) rho],  rho = -i G1 (one spin projection;
+//        h from HF.h:57-104 at U_eff, h0 = h at U = 0),
+//   Ec = -Re sum_{p,q} (w_xx(p,q) G2xx[p q; p q] + w_xy(p,q) G2xy[p q; p q])
+// with the pair weights of the collision integral (collision_integral.h:41-62):
+// on one site w_xy = U and w_xx = U for different bands (0 for p = q); between
+// sites m apart w = V_m = U law[m-1].  G2_t[p q; p q] = D[t][(p n + p) n + q].
+// One block: out = {E1 + Ec, 2 Tr[h0 rho], Tr[(h - h0) rho], Ec}.
+constexpr int kEnergyThreads = 256;
+static __global__ void __launch_bounds__(kEnergyThreads) k_energy(Dev d, StageP st, double *out)
+{
+    __shared__ double2 gd[kMaxN];
+    __shared__ double red[3][kEnergyThreads];
+    const int n = d.n, Ns = d.Ns;
+    const double2 *G = d.Y1;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) gd[p] = G[p * (n + 1)];
+    __syncthreads();
+    StageP st0 = st;
+    st0.U = 0.0;
+    double e0 = 0.0, eh = 0.0, ec = 0.0;
+    for (int x = threadIdx.x; x < n * n; x += blockDim.x) {
+        const int mu = x / n, nu = x % n;
+        const double2 rho = c_mi(G[nu * n + mu]);  // rho[nu][mu]
+        const double2 h = h_entry(d, G, gd, mu, nu, st);
+        const double2 h0 = h_entry(d, G, gd, mu, nu, st0);
+        e0 += 2.0 * (h0.x * rho.x - h0.y * rho.y);
+        eh += (h.x - h0.x) * rho.x - (h.y - h0.y) * rho.y;
+        const int i = mu % Ns, a = mu / Ns, j = nu % Ns, b = nu / Ns;
+        const int m = abs(i - j);
+        double wxx = 0.0, wxy = 0.0;
+        if (m == 0) {
+            wxy = st.U;
+            wxx = (a != b) ? st.U : 0.0;
+        } else if (m <= d.nv) {
+            wxx = wxy = st.U * d.law[m - 1];
+        }
+        const long long q = ((long long)mu * n + mu) * n + nu;
+        ec -= wxx * d.D[q].x + wxy * d.D[d.n3 + q].x;
+    }
+    red[0][threadIdx.x] = e0;
+    red[1][threadIdx.x] = eh;
+    red[2][threadIdx.x] = ec;
+    __syncthreads();
+    for (int w = kEnergyThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w)
+            for (int c = 0; c < 3; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = red[0][0] + red[1][0] + red[2][0];
+        out[1] = red[0][0];
+        out[2] = red[1][0];
+        out[3] = red[2][0];
+    }
+}
+
 // reference IDX_8D layout <-> device orbital layout
 __device__ __forceinline__ long long ref_index(int Ns, int Nb, long long x, int n)
 {

@@ -46,6 +46,12 @@ struct SymDev {
     int *err;               // device error word (bounded waits)
 };
 
+// bulk prefetch of a contiguous range into L2 (16-byte aligned, size a multiple of 16)
+__device__ __forceinline__ void l2_prefetch_bulk(const void *p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // stage k reads TMPb (k even) or TMPa (k odd) and writes the other one
 __device__ __forceinline__ const float *sym_in(const SymDev &s, int k) { return (k & 1) ? s.TMPa : s.TMPb; }
 __device__ __forceinline__ float *sym_out(const SymDev &s, int k) { return (k & 1) ? s.TMPb : s.TMPa; }
@@ -114,6 +120,13 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
 {
     if (!*s.d.active) return;
     const Dev &d = s.d;
+    if (threadIdx.x == 0) {
+        // the block's FP64 state tiles (16 KB each, contiguous) do not depend on
+        // the GEMM: start them towards L2 before anything else
+        const long long tile = ((long long)blockIdx.y * s.npairs + blockIdx.x) * kTB * kTB;
+        l2_prefetch_bulk(s.Yc + tile, kTB * kTB * sizeof(double2));
+        if (k > 0) l2_prefetch_bulk(s.Ac + tile, kTB * kTB * sizeof(double2));
+    }
     constexpr int n = NN;
     constexpr int GLD = NN + 1;   // padded G1 rows (bank-conflict-free column reads)
     constexpr int KLD = kTB + 1;  // padded K rows

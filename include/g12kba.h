@@ -143,6 +143,18 @@ int g12_rhs(g12_ctx *ctx, const double *G1, const double *G2xx, const double *G2
             double U_eff, double w_quench, int32_t Nq_eff,
             double *h, double *comm1, double *Ix, double *K1, double *K2xx, double *K2xy);
 
+/* Total energy of the context's current state, reduced on the GPU in FP64.
+ * No counterpart in the reference; it is the energy the G1-G2 equations
+ * conserve while h0 and U are constant (no quench ramp, after adiabatic
+ * switching):
+ *   E = 2 Tr[h0 rho] + Tr[(h - h0) rho]
+ *       - Re sum_{p,q} (w_xx(p,q) G2xx[p q; p q] + w_xy(p,q) G2xy[p q; p q]),
+ * rho = -i G1, h = HF.h:57-104 at (U_eff, w_quench, Nq_eff), h0 = h at U = 0,
+ * w the pair interaction of collision_integral.h:41-62 (U on one site, 0
+ * for the same orbital in xx; V_m = U_eff law(m) between sites m apart).
+ * E_out[4] = {E, 2 Tr[h0 rho], Tr[(h - h0) rho], correlation part}. */
+int g12_total_energy(g12_ctx *ctx, double U_eff, double w_quench, int32_t Nq_eff, double *E_out);
+
 /* Device time of the last g12_propagate* call's kernels (CUDA events, ms). */
 double g12_last_device_ms(const g12_ctx *ctx);
 

@@ -325,6 +325,57 @@ def run_reference_exe(cfg: Config, workdir, g0=None, skip_as=False, no_text=True
     return out
 
 
+def pair_index(Ns, Nb):
+    """[p, q] -> IDX_8D position of G2[p q; p q] (commutators.h:60 with
+    mu1 = nu1 = p = (i, a), mu2 = nu2 = q = (j, b))."""
+    n = Ns * Nb
+    mu = np.arange(n)
+    s, b = mu % Ns, mu // Ns
+    i, a = s[:, None], b[:, None]
+    j, bb = s[None, :], b[None, :]
+    Ns2, Nb2 = Ns * Ns, Nb * Nb
+    return (i + j * Ns) + (a + bb * Nb) * Ns2 + (i + j * Ns) * Ns2 * Nb2 + (a + bb * Nb) * Ns2 * Ns2 * Nb2
+
+
+def pair_weights(cfg: Config, U):
+    """Pair interaction (w_xx, w_xy)[p, q] of the collision integral
+    (collision_integral.h:41-62): on one site U (w_xx: different bands only),
+    between sites m apart V_m (AS.h:136-140 law at U)."""
+    n, Ns = cfg.n, cfg.Ns
+    mu = np.arange(n)
+    s, b = mu % Ns, mu // Ns
+    d = np.abs(s[:, None] - s[None, :])
+    V = cfg.vvec(U)
+    Vd = np.zeros((n, n))
+    for m in range(1, len(V) + 1):
+        Vd[d == m] = V[m - 1]
+    wxy = np.where(d == 0, U, Vd)
+    wxx = np.where(d == 0, np.where(b[:, None] != b[None, :], U, 0.0), Vd)
+    return wxx, wxy
+
+
+def total_energy(o: "_Lib", cfg: Config, G1, G2xx, G2xy, U=None, w_quench=0.0, Nq=0):
+    """Total energy [E, 2 Tr[h0 rho], Tr[(h - h0) rho], correlation part] of a
+    state (G2 in the IDX_8D layout).  The reference computes none: this is the
+    energy its equations conserve while h0 and U are constant, with h from the
+    restated HF.h:57-104 (h0: the same at G1 = 0) and the pair weights of
+    collision_integral.h:41-62:
+        E = 2 Tr[h0 rho] + Tr[(h - h0) rho] - Re sum w_xx G2xx[pq;pq] + w_xy G2xy[pq;pq]."""
+    U = cfg.U if U is None else U
+    n = cfg.n
+    G1 = _c(G1, (n, n))
+    V = cfg.vvec(U)
+    h = o.h_hf(G1, cfg.Ns, cfg.Nb, U, cfg.t1, cfg.t2, w_quench, V, Nq)
+    h0 = o.h_hf(np.zeros((n, n), np.complex128), cfg.Ns, cfg.Nb, U, cfg.t1, cfg.t2, w_quench, V, Nq)
+    rho = -1j * G1
+    e0 = 2.0 * np.trace(h0 @ rho).real
+    eh = np.trace((h - h0) @ rho).real
+    wxx, wxy = pair_weights(cfg, U)
+    I = pair_index(cfg.Ns, cfg.Nb)
+    ec = -float(np.sum(wxx * np.asarray(G2xx)[I].real + wxy * np.asarray(G2xy)[I].real))
+    return np.array([e0 + eh + ec, e0, eh, ec])
+
+
 def idx8_to_orbital(Ns, Nb):
     """Permutation p with orbital_flat = ref_flat[p] where orbital_flat is
     indexed nu1 + n*nu2 + n^2*mu1 + n^3*mu2 (mu = site + band*Ns)."""

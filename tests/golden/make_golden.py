@@ -7,6 +7,7 @@ oracle/_ref/g12_ref for full Main.cpp runs).  Inputs are seeded random
 complex arrays or the physics configurations listed below.
 
 Run from the repository root:  python tests/golden/make_golden.py
+(``python tests/golden/make_golden.py energy`` writes energy_pin.npz alone).
 """
 import os
 import sys
@@ -100,6 +101,39 @@ def full_runs():
         print(name, "T =", traj.shape[0], "max|G2| =", float(np.max(np.abs(r["g2xx"]))))
 
 
+# total-energy pin: the state after adiabatic switching and the state after the
+# T RK4 iterations of a run (constant U, quench masked by the t < 50 gate), at
+# two step sizes over the same simulated time
+ENERGY_PIN = {
+    "dt02": Config(Ns=4, Nb=2, Nq=1, time_steps=150, U=1.5, t1=1.0, t2=0.3, dt=0.02, EHM=True,
+                    vlaw="inv", q_type="full", quench_strength=1.0, AS_rate=0.5, AS_midpoint=3),
+    "dt01": Config(Ns=4, Nb=2, Nq=1, time_steps=300, U=1.5, t1=1.0, t2=0.3, dt=0.01, EHM=True,
+                    vlaw="inv", q_type="full", quench_strength=1.0, AS_rate=0.5, AS_midpoint=3),
+}
+
+
+def energy_pin():
+    """G1 and both G2 at the same time: the final G2 of a run of T steps and
+    G1 at index T of a longer run of the same input (both runs take the same
+    steps up to T)."""
+    import dataclasses
+    out = {}
+    for tag, cfg in ENERGY_PIN.items():
+        with tempfile.TemporaryDirectory() as d:
+            a = run_reference_exe(cfg, d)
+        T = a["traj"].shape[0]  # while (t < tmax) iterations (RK_solver.h:96)
+        longer = dataclasses.replace(cfg, time_steps=cfg.time_steps + 3)
+        with tempfile.TemporaryDirectory() as d:
+            b = run_reference_exe(longer, d)
+        assert np.array_equal(a["traj"], b["traj"][:T])
+        out[f"{tag}/g1_0"], out[f"{tag}/g2xx_0"], out[f"{tag}/g2xy_0"] = a["g1_as"], a["g2xx_as"], a["g2xy_as"]
+        out[f"{tag}/g1_T"], out[f"{tag}/g2xx_T"], out[f"{tag}/g2xy_T"] = b["traj"][T], a["g2xx"], a["g2xy"]
+        out[f"{tag}/T"] = np.array(T)
+        for k, v in cfg.__dict__.items():
+            out[f"{tag}/cfg_{k}"] = np.array(v)
+    np.savez_compressed(os.path.join(OUT, "energy_pin.npz"), **out)
+
+
 def sample_input():
     """The reference's only fixture (G12KBA-GW/input), kept verbatim as test
     data for the input reader."""
@@ -111,6 +145,10 @@ def sample_input():
 if __name__ == "__main__":
     if not Reference.available():
         sys.exit("build the compiled reference first: oracle/build_ref.sh")
+    if sys.argv[1:] == ["energy"]:
+        energy_pin()
+        sys.exit(0)
     per_routine(Reference())
     full_runs()
+    energy_pin()
     sample_input()

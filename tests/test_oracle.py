@@ -103,3 +103,55 @@ def test_full_run_vs_live_reference(oracle, reference):
     traj, G1, XX, XY = oracle.run(cfg, r["g0"])
     assert rel_err(traj, r["traj"]) <= 1e-12
     assert rel_err(XY, r["g2xy"]) <= 1e-11
+
+
+def energy_pin_case(tag):
+    """(Config, state after adiabatic switching, state after T RK4 iterations)
+    of tests/golden/energy_pin.npz (outputs of the reference's own runs)."""
+    g = load_golden("energy_pin.npz")
+    pre = tag + "/cfg_"
+    cfg = Config(**{k[len(pre):]: g[k].item() for k in g.files if k.startswith(pre)})
+    s0 = tuple(g[f"{tag}/{k}_0"] for k in ("g1", "g2xx", "g2xy"))
+    sT = tuple(g[f"{tag}/{k}_T"] for k in ("g1", "g2xx", "g2xy"))
+    return cfg, s0, sT, int(g[tag + "/T"])
+
+
+def test_total_energy_conserved_by_reference_runs(oracle):
+    """The total energy is conserved along the reference's own trajectories to
+    RK4 truncation: the drift falls 16x when dt halves, while the correlation
+    part alone moves by ~0.08."""
+    from oracle import total_energy
+    drift = {}
+    for tag in ("dt02", "dt01"):
+        cfg, s0, sT, T = energy_pin_case(tag)
+        E0, ET = total_energy(oracle, cfg, *s0), total_energy(oracle, cfg, *sT)
+        drift[tag] = abs(ET[0] - E0[0])
+        assert abs(ET[3] - E0[3]) > 0.05
+        assert drift[tag] <= 1e-9 * abs(E0[0]), drift
+    assert drift["dt01"] <= drift["dt02"] / 8, drift
+
+
+def test_total_energy_sign_matters(oracle):
+    """A planted mistake in the oracle's functional (the correlation part with
+    the wrong sign, or left out) is not conserved: the pin has teeth."""
+    from oracle import total_energy
+    cfg, s0, sT, _ = energy_pin_case("dt01")
+    E0, ET = total_energy(oracle, cfg, *s0), total_energy(oracle, cfg, *sT)
+    flipped = (ET[1] + ET[2] - ET[3]) - (E0[1] + E0[2] - E0[3])
+    dropped = (ET[1] + ET[2]) - (E0[1] + E0[2])
+    assert abs(flipped) > 0.1 and abs(dropped) > 0.05
+
+
+def test_total_energy_oracle_steps(oracle):
+    """The restated RK4 conserves the same functional from the pinned state."""
+    from oracle import total_energy
+    cfg, s0, _, _ = energy_pin_case("dt01")
+    G1, XX, XY = (np.array(a, dtype=np.complex128) for a in s0)
+    E0 = total_energy(oracle, cfg, G1, XX, XY)
+    t, tt = 0.0, 0.0
+    for _ in range(40):
+        tt = oracle.step(cfg, 1, t, tt, G1, XX, XY)
+        t += cfg.dt
+    E = total_energy(oracle, cfg, G1, XX, XY)
+    assert abs(E[0] - E0[0]) <= 1e-11 * abs(E0[0])
+    assert abs(E[3] - E0[3]) > 1e-3
