@@ -340,7 +340,8 @@ class Context:
         avg = np.zeros(16)
         calls = (C.c_int32 * 16)()
         nk = _check(lib().g12_kernel_times(self.h, nsteps, _ptr(avg), calls, 16), self.h)
-        return {lib().g12_kernel_name(self.h, i).decode(): (float(avg[i]), int(calls[i])) for i in range(nk)}
+        return {lib().g12_kernel_name(self.h, i).decode(): (float(avg[i]), int(calls[i]))
+                for i in range(nk) if calls[i]}
 
 
 class Batch:

@@ -214,6 +214,13 @@ void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
     k_step_begin<<<1, 256, 0, s>>>(d);
     for (int k = 0; k < 4; ++k) {
         k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, s>>>(d, k);
+        if (ctx->prec != G12_PREC_FP64 && d.gate && mixed_fuses_g1(ctx->mixed)) {
+            // digit GEMM, then the epilogue with the G1 side as extra blocks of
+            // its launch (two launches per stage after k_prep)
+            mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, 0, s);
+            mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, 1, s, true);
+            continue;
+        }
         if (ctx->prec != G12_PREC_FP64 && d.gate) {
             // symmetric engine: k_g1 forks after the GEMM (one 201 KB CTA per SM,
             // which k_g1's blocks would keep off their SMs) and overlaps the epilogue
@@ -739,14 +746,16 @@ extern "C" int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms
         timed(0, [&] { k_step_begin<<<1, 256, 0, ctx->s>>>(d); });
         for (int k = 0; k < 4; ++k) {
             timed(1, [&] { k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, ctx->s>>>(d, k); });
-            timed(2, [&] { k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s>>>(d, k); });
+            // the digit-GEMM path runs the G1 side inside its epilogue launch
+            const bool fused = ctx->prec != G12_PREC_FP64 && d.gate && mixed_fuses_g1(ctx->mixed);
+            if (!fused) timed(2, [&] { k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s>>>(d, k); });
             if (!d.gate) continue;
             if (ctx->prec == G12_PREC_FP64) {
                 timed(3, [&] { k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, ctx->s>>>(d, k, lc.ab); });
                 timed(4, [&] { k_apply<true><<<lc.apply_grid, lc.cd_threads, lc.cd_smem, ctx->s>>>(d, k, lc.cd); });
             } else {
                 for (int q = 0; q < mixed_kernel_kinds(ctx->mixed); ++q)
-                    timed(3 + q, [&] { mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, q, ctx->s); });
+                    timed(3 + q, [&] { mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, q, ctx->s, fused); });
             }
         }
         if (ctx->evict_bytes) cudaMemsetAsync(ctx->evict_buf, 0, ctx->evict_bytes, ctx->s);
@@ -813,7 +822,10 @@ extern "C" double g12_fp64_peak_tflops(int32_t device)
 extern "C" int32_t g12_launches_per_step(const g12_ctx *ctx)
 {
     if (!ctx) return 0;
-    int per_stage = 2;
-    if (ctx->d.gate) per_stage += (ctx->prec == G12_PREC_FP64) ? 2 : mixed_launches_per_stage(ctx->mixed);
+    int per_stage = 2;  // k_prep, k_g1
+    if (ctx->d.gate) {
+        per_stage += (ctx->prec == G12_PREC_FP64) ? 2 : mixed_launches_per_stage(ctx->mixed);
+        if (ctx->prec != G12_PREC_FP64 && mixed_fuses_g1(ctx->mixed)) per_stage -= 1;  // k_g1 in k_sym_epi
+    }
     return 1 + 4 * per_stage;
 }

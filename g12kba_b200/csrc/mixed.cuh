@@ -145,6 +145,7 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
     s.gemm_partner = gp;
     s.pairs = pp;
     m.epi_smem = size_t(n) * (n + 1) * sizeof(double2) + 2 * kTB * (kTB + 1) * sizeof(float2) + kTB * (kTB + 1) * sizeof(double2);
+    m.epi_smem = std::max(m.epi_smem, g1_smem(n2));  // G1-side blocks of k_sym_epi
     m.simt_smem = (size_t(128) * 2 * n + size_t(128) * (2 * n + 1)) * sizeof(float) + size_t(n2) * sizeof(float2);
     cudaFuncSetAttribute(k_sym_epi<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
     cudaFuncSetAttribute(k_sym_epi<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
@@ -239,9 +240,15 @@ inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t sme
     cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
-inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, cudaStream_t st)
+// whether k_sym_epi runs the stage's G1 side itself (the digit-GEMM path)
+inline bool mixed_fuses_g1(const MixedState &m) { return m.tc && m.oz2; }
+
+// q = 0: the W contraction, q = 1: the stage epilogue; fuse_g1 (digit-GEMM
+// path only) adds the G1-side blocks to the epilogue launch
+inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, cudaStream_t st, bool fuse_g1 = false)
 {
     m.s.d = d;
+    m.s.g1x = 0;
     const SymDev &s = m.s;
     if (q == 0) {
         if (m.tc) {
@@ -259,6 +266,14 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
         }
     } else {
         const dim3 g(s.npairs, 2);
+        if (m.oz2 && m.tc) {
+            SymDev sf = s;
+            sf.g1x = fuse_g1 ? int((s.d.n2 + 255) / 256) : 0;
+            const dim3 gf(s.npairs + sf.g1x, 2);
+            if (s.n == 32) launch_pdl(k_sym_epi<32>, gf, dim3(256), m.epi_smem, st, sf, k);
+            else launch_pdl(k_sym_epi<16>, gf, dim3(256), m.epi_smem, st, sf, k);
+            return;
+        }
         if (s.n == 32 && m.oz2) launch_pdl(k_sym_epi<32>, g, dim3(256), m.epi_smem, st, s, k);
         else if (s.n == 16 && m.oz2) launch_pdl(k_sym_epi<16>, g, dim3(256), m.epi_smem, st, s, k);
         else if (s.n == 32) k_sym_epi<32><<<g, 256, m.epi_smem, st>>>(s, k);

@@ -44,6 +44,8 @@ struct SymDev {
     const int *gemm_partner;// [gemm_tiles][cpt] slot of cbar in the same tile
     const int2 *pairs;      // [npairs] (Rb, Cb), Rb <= Cb
     int *err;               // device error word (bounded waits)
+    int g1x;                // k_sym_epi blocks past the tile pairs (blockIdx.y = 0) that run
+                            // the stage's G1 side (g1_body); 0: k_g1 is launched on its own
 };
 
 // bulk prefetch of a contiguous range into L2 (16-byte aligned, size a multiple of 16)
@@ -120,6 +122,14 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
 {
     if (!*s.d.active) return;
     const Dev &d = s.d;
+    if (blockIdx.x >= s.npairs) {
+        // the stage's G1 side, folded into this launch (h and Ix come from k_prep)
+        if (blockIdx.y == 0 && blockIdx.x - s.npairs < s.g1x) {
+            grid_dep_wait();
+            g1_body(d, k, blockIdx.x - s.npairs);
+        }
+        return;
+    }
     if (threadIdx.x == 0) {
         // the block's FP64 state tiles (16 KB each, contiguous) do not depend on
         // the GEMM: start them towards L2 before anything else
