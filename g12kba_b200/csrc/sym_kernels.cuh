@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) k_sym_gemm_simt(SymDev s, int k)
 // RK4 bookkeeping on the compressed state, next-stage input (both tiles, FP32),
 // particle-2 diagonal D (FP64).
 template <int NN>
-__global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
+__global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
 {
     if (!*s.d.active) return;
     const Dev &d = s.d;
@@ -188,31 +188,36 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
     if constexpr (NN >= kTB) {
         // n >= 32: every 32 x 32 tile has one mu2 (rows) and one nu2 (columns),
         // so the site weights, Rt, the Pi factor Q and (for xx) the three-G1
-        // products of Psi are 32-entry vectors of mu1 or nu1 (staged below).
-        __shared__ double wa[kTB], wb[kTB];
-        __shared__ double2 ra[kTB], rb[kTB], qa[kTB], qb[kTB];
-        __shared__ double2 x1[kTB], y1[kTB], x2[kTB], y2[kTB], fa[kTB], hb[kTB];
+        // products of Psi are 32-entry vectors of mu1 or nu1.  A thread keeps
+        // one row rl = lane (e = threadIdx.x + 256 j), so the mu1 vectors live
+        // in its registers and the nu1 vectors are warp-uniform shared reads.
+        __shared__ double wb[kTB];
+        __shared__ double2 rb[kTB], qb[kTB], y1[kTB], y2[kTB], hb[kTB];
         const int mu2 = R0 / n, m0 = R0 % n, nu2 = C0 / n, c0 = C0 % n;
         const int sj = site[mu2], sl = site[nu2];
+        const double2 *Rt2 = d.Rt + ((long long)mu2 * n + nu2) * Ns;
+        const long long q2 = ((long long)nu2 * n + mu2) * n;
         if (threadIdx.x < kTB) {
-            const int l = threadIdx.x, mu1 = m0 + l, nu1 = c0 + l;
-            const int si = site[mu1], sk = site[nu1];
-            wa[l] = U * double(si == sj) + vdist(si, sj);
+            const int l = threadIdx.x, nu1 = c0 + l;
+            const int sk = site[nu1];
             wb[l] = U * double(sk == sl) + vdist(sk, sl);
-            const double2 *Rt2 = d.Rt + ((long long)mu2 * n + nu2) * Ns;
-            ra[l] = Rt2[si];
             rb[l] = Rt2[sk];
-            const long long q2 = ((long long)nu2 * n + mu2) * n;
-            qa[l] = Qo[q2 + mu1];
             qb[l] = Qo[q2 + nu1];
             if (t == 0) {
-                x1[l] = Gs[mu1 * GLD + mu2];
                 y1[l] = Gs[mu2 * GLD + nu1];
-                x2[l] = Gs[mu1 * GLD + nu2];
                 y2[l] = Gs[nu2 * GLD + nu1];
-                fa[l] = c_mul(Gs[mu2 * GLD + mu1], Gs[mu1 * GLD + nu2]);
                 hb[l] = c_mul(Gs[mu2 * GLD + nu1], Gs[nu1 * GLD + nu2]);
             }
+        }
+        const int rl = threadIdx.x & (kTB - 1);
+        const int mu1 = m0 + rl, si = site[mu1];
+        const double wa = U * double(si == sj) + vdist(si, sj);
+        const double2 ra = Rt2[si], qa = Qo[q2 + mu1];
+        double2 x1 = make_double2(0.0, 0.0), x2 = x1, fa = x1;
+        if (t == 0) {
+            x1 = Gs[mu1 * GLD + mu2];
+            x2 = Gs[mu1 * GLD + nu2];
+            fa = c_mul(Gs[mu2 * GLD + mu1], Gs[mu1 * GLD + nu2]);
         }
         __syncthreads();
         const double2 g22 = Gs[mu2 * GLD + nu2];
@@ -221,26 +226,27 @@ __global__ void __launch_bounds__(256) k_sym_epi(SymDev s, int k)
         const double2 *RttJ = Rtt + (long long)sj * n * n, *RttL = Rtt + (long long)sl * n * n;
         const double2 *QtM = Qt + (long long)mu2 * n * n, *QtN = Qt + (long long)nu2 * n * n;
 #pragma unroll 4
-        for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
-            const int rl = e % kTB, cl = e / kTB;
-            const int mu1 = m0 + rl, nu1 = c0 + cl;
+        for (int j = 0; j < kTB * kTB / 256; ++j) {
+            const int cl = (threadIdx.x >> 5) + 8 * j;
+            const int e = cl * kTB + rl;  // = threadIdx.x + 256 j
+            const int nu1 = c0 + cl;
             const float2 w1 = Wrc[cl * (kTB + 1) + rl];
             const float2 w2 = Wcr[rl * (kTB + 1) + cl];
             const double2 C = make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
             const double2 g11 = Gs[mu1 * GLD + nu1];
             const double2 g1122 = c_mul(g11, g22);
-            const double wd = wa[rl] - wb[cl];
+            const double wd = wa - wb[cl];
             double2 psi = c_scale(g1122, wd);
             psi = c_add(psi, c_i(c_mul(g22, c_sub(RttJ[nu1 * n + mu1], RttL[nu1 * n + mu1]))));
-            psi = c_add(psi, c_i(c_mul(g11, c_sub(ra[rl], rb[cl]))));
+            psi = c_add(psi, c_i(c_mul(g11, c_sub(ra, rb[cl]))));
             if (t == 0) {
                 psi = c_sub(psi, c_scale(g1122, U * (double(mu1 == mu2) - double(nu1 == nu2))));
-                const double2 e1 = c_sub(c_mul(x1[rl], y1[cl]), c_mul(x2[rl], y2[cl]));
-                const double2 e2 = c_sub(fa[rl], hb[cl]);
+                const double2 e1 = c_sub(c_mul(x1, y1[cl]), c_mul(x2, y2[cl]));
+                const double2 e2 = c_sub(fa, hb[cl]);
                 psi = c_add(psi, c_scale(c_mi(c_add(c_mul(g22, e1), c_mul(g11, e2))), U));
             }
             const double2 pi = c_mul(g22, c_sub(QtM[nu1 * n + mu1], QtN[nu1 * n + mu1]));
-            const double2 piP = c_mul(Gs[nu1 * GLD + mu1], c_sub(qb[cl], qa[rl]));
+            const double2 piP = c_mul(Gs[nu1 * GLD + mu1], c_sub(qb[cl], qa));
             const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
             if (fused) {
                 // RK4 bookkeeping of this element right away (off-diagonal tile pairs)
