@@ -378,15 +378,31 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                 }
                 float v[HF];
                 const unsigned char *row = As + sa * Sh::A_STAGE + m * 128;
+                // n = 32: the two halves of a row sit at the same chunk of two
+                // 128-byte boxes; the second half reads its chunks in the order
+                // q4 ^ 4 so that one load instruction touches 8 distinct chunks of
+                // the 4 rows of a quarter-warp (no bank conflict), and swaps back
+                constexpr int HX = (HF / 4 == 8) ? 4 : 0;
+                const int hx = half ? HX : 0;
 #pragma unroll
                 for (int q4 = 0; q4 < HF / 4; ++q4) {
-                    const int f = half * HF + 4 * q4;            // first FP32 index of this 16-byte chunk
+                    const int f = half * HF + 4 * (q4 ^ hx);     // first FP32 index of this 16-byte chunk
                     const int kb = f >> 5, j = (f & 31) >> 2;
                     const float4 q = *reinterpret_cast<const float4 *>(row + kb * 128 * 128 + ((j ^ sw) << 4));
                     v[4 * q4 + 0] = q.x;
                     v[4 * q4 + 1] = q.y;
                     v[4 * q4 + 2] = q.z;
                     v[4 * q4 + 3] = q.w;
+                }
+                if constexpr (HX != 0) {
+                    if (half) {
+#pragma unroll
+                        for (int x = 0; x < HF / 2; ++x) {
+                            const float tmp = v[x];
+                            v[x] = v[x + HF / 2];
+                            v[x + HF / 2] = tmp;
+                        }
+                    }
                 }
                 mbar_arrive(&empty_a[sa]);
                 float mx = 0.f;
