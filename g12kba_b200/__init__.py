@@ -140,6 +140,8 @@ def lib():
         L.g12_mlp_adam.argtypes = [_vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]
         L.g12_mlp_set_norm.argtypes = [_vp, C.c_int32, C.c_int32, C.c_int32, _fp, C.c_float, C.c_float, C.c_float]
         L.g12_mlp_windows.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, _vp, _vp]
+        L.g12_mlp_grad_windows.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, _dp]
+        L.g12_mlp_grad_buffer.argtypes = [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]
         L.g12_mlp_train_windows.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, C.c_float, C.c_float,
                                             _dp]
         L.g12_mlp_train_pushforward.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, C.c_int32,

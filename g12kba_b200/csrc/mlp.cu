@@ -395,6 +395,8 @@ struct g12_mlp {
     long long adam_t = 0;
     float *scratch = nullptr;
     long long scratch_floats = 0;
+    float *grad_all = nullptr;     // every gW / gb segment, each padded to 64 floats
+    long long grad_floats = 0;
     long long *idx2_d = nullptr;
     unsigned long long noise_ctr = 0;
     std::vector<void *> allocs;
@@ -551,10 +553,26 @@ extern "C" int g12_mlp_create(const int32_t *dims, int32_t max_batch, uint64_t s
     m->A.resize(4);
     m->dA.resize(4);
     std::mt19937_64 rng(seed);
+    // the gradients live in one block (one collective reduces all of them in
+    // data-parallel training); segments start on 256-byte boundaries and the
+    // padding stays zero
+    auto pad64 = [](size_t x) { return (x + 63) / 64 * 64; };
+    size_t gtot = 0;
+    for (int l = 0; l < 4; ++l) gtot += pad64(size_t(dims[l]) * dims[l + 1]) + pad64(size_t(dims[l + 1]));
+    if (!malloc_zero(m, &m->grad_all, gtot)) return fail(G12_ERR_NOMEM, "out of device memory (MLP)");
+    m->grad_floats = (long long)gtot;
+    size_t goff = 0;
     for (int l = 0; l < 4; ++l) {
         const size_t nw = size_t(dims[l]) * dims[l + 1], nb = dims[l + 1];
-        if (!malloc_zero(m, &m->W[l], nw) || !malloc_zero(m, &m->b[l], nb) || !malloc_zero(m, &m->gW[l], nw) ||
-            !malloc_zero(m, &m->gb[l], nb) || !malloc_zero(m, &m->mW[l], nw) || !malloc_zero(m, &m->vW[l], nw) ||
+        m->gW[l] = m->grad_all + goff;
+        goff += pad64(nw);
+        m->gb[l] = m->grad_all + goff;
+        goff += pad64(nb);
+    }
+    for (int l = 0; l < 4; ++l) {
+        const size_t nw = size_t(dims[l]) * dims[l + 1], nb = dims[l + 1];
+        if (!malloc_zero(m, &m->W[l], nw) || !malloc_zero(m, &m->b[l], nb) ||
+            !malloc_zero(m, &m->mW[l], nw) || !malloc_zero(m, &m->vW[l], nw) ||
             !malloc_zero(m, &m->mb[l], nb) || !malloc_zero(m, &m->vb[l], nb) ||
             !malloc_zero(m, &m->Z[l], size_t(max_batch) * dims[l + 1]) ||
             !malloc_zero(m, &m->A[l], size_t(max_batch) * dims[l + 1]) ||
@@ -736,6 +754,32 @@ extern "C" int g12_mlp_train_windows(g12_mlp *m, const float *feat_dev, int32_t 
     int rc = g12_mlp_loss_grad(m, m->Xbuf, m->Ybuf, batch, loss);
     if (rc) return rc;
     return g12_mlp_adam(m, lr, 0.9f, 0.999f, 1e-8f, weight_decay);
+}
+
+// windows, loss and gradients without the Adam step (data-parallel training
+// reduces the gradients across ranks in between)
+extern "C" int g12_mlp_grad_windows(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t snaps, const int64_t *idx,
+                                    int32_t batch, double *loss)
+{
+    if (!m || !m->has_norm || !feat_dev || !idx || batch < 128 || batch % 128 || batch > m->max_batch)
+        return G12_ERR_INVALID;
+    MCK(cudaSetDevice(m->device));
+    if (!windows_in_range(m, ntraj, snaps, idx, batch)) {
+        m->err = "window out of the trajectory";
+        return G12_ERR_INVALID;
+    }
+    MCK(cudaMemcpyAsync(m->idx_d, idx, sizeof(long long) * 2 * batch, cudaMemcpyHostToDevice, m->s));
+    k_windows<<<dim3(64, batch), 256, 0, m->s>>>(feat_dev, snaps, m->idx_d, batch, m->norm, m->Xbuf, m->Ybuf);
+    MCK(cudaGetLastError());
+    return g12_mlp_loss_grad(m, m->Xbuf, m->Ybuf, batch, loss);
+}
+
+extern "C" int g12_mlp_grad_buffer(g12_mlp *m, float **grads_dev, int64_t *count)
+{
+    if (!m || !grads_dev || !count) return G12_ERR_INVALID;
+    *grads_dev = m->grad_all;
+    *count = m->grad_floats;
+    return G12_OK;
 }
 
 // network inputs and targets of windows (host copies; for tests)

@@ -198,6 +198,28 @@ class MLP:
                                               weight_decay, C.byref(loss)))
         return loss.value
 
+    def grad_windows(self, feat, idx):
+        """Loss and gradients of one batch of windows, no Adam step (the
+        gradients are complete on the device when this returns)."""
+        idx = np.ascontiguousarray(idx, np.int64)
+        loss = C.c_double()
+        self._chk(lib().g12_mlp_grad_windows(self.h, C.c_void_p(feat.data_ptr()), feat.shape[0], feat.shape[1],
+                                             idx.ctypes.data_as(C.POINTER(C.c_int64)), idx.shape[0],
+                                             C.byref(loss)))
+        return loss.value
+
+    def grad_tensor(self):
+        """The device block of all gradients as a float32 torch tensor (a view:
+        writes to it change the gradients the next Adam step uses)."""
+        ptr, cnt = C.c_void_p(), C.c_int64()
+        self._chk(lib().g12_mlp_grad_buffer(self.h, C.byref(ptr), C.byref(cnt)))
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (cnt.value,), "typestr": "<f4", "data": (ptr.value, False),
+                                        "version": 2}
+
+        return _torch().as_tensor(_View(), device=f"cuda:{self.device}")
+
     def train_pushforward(self, feat, idx, r, lr, noise=0.0, weight_decay=0.0):
         idx = np.ascontiguousarray(idx, np.int64)
         loss = C.c_double()
@@ -213,6 +235,56 @@ class MLP:
         self._chk(lib().g12_mlp_rollout(self.h, C.c_void_p(feat.data_ptr()), feat.shape[0], feat.shape[1], t0,
                                         C.byref(ms)))
         return ms.value
+
+
+def average_gradients(grad, pg=None):
+    """In place: the mean of ``grad`` over the ranks of ``pg`` (all-reduce of
+    the sum, then 1/world), the data-parallel step between the ranks'
+    backward passes and their identical Adam steps."""
+    import torch.distributed as dist
+    world = dist.get_world_size(pg)
+    if world > 1:
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=pg)
+        grad.mul_(1.0 / world)
+    return grad
+
+
+def broadcast_from_root(t, pg=None):
+    """In place: rank 0's ``t`` on every rank of ``pg``."""
+    import torch.distributed as dist
+    if dist.get_world_size(pg) > 1:
+        dist.broadcast(t, src=dist.get_global_rank(pg, 0) if pg is not None else 0, group=pg)
+    return t
+
+
+def train_data_parallel(mlp, feat, steps, lo, hi, pg=None, batch=512, lr=1e-3, lr_min=1e-5, weight_decay=0.0,
+                        seed=0, log=None):
+    """Data-parallel Adam over the ranks of ``pg``: every rank draws its own
+    windows (t in [lo, hi)) from its own trajectories ``feat``, the gradients
+    are averaged across ranks (one all-reduce of the gradient block per step)
+    and every rank takes the same Adam step, so the parameters stay equal
+    (rank 0's initial parameters are broadcast first).  ``mlp`` provides
+    get_params / set_params / grad_windows / grad_tensor / adam.  Returns this
+    rank's loss history."""
+    import torch.distributed as dist
+    torch = _torch()
+    rank = dist.get_rank(pg)
+    p0 = torch.as_tensor(np.asarray(mlp.get_params(), np.float32), device=feat.device)
+    mlp.set_params(broadcast_from_root(p0, pg).cpu().numpy())
+    rng = np.random.default_rng([seed, rank])
+    ntraj = feat.shape[0]
+    hist = []
+    for it in range(steps):
+        a = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * it / max(1, steps)))
+        idx = np.stack([rng.integers(0, ntraj, batch), rng.integers(lo, hi, batch)], axis=1)
+        hist.append(mlp.grad_windows(feat, idx))
+        g = average_gradients(mlp.grad_tensor(), pg)
+        if g.is_cuda:
+            torch.cuda.current_stream(g.device).synchronize()  # the reduction ran on torch's stream
+        mlp.adam(a, weight_decay=weight_decay)
+        if log and (it % max(1, steps // 20) == 0 or it == steps - 1):
+            log(f"rank {rank} step {it} lr {a:.2e} loss {hist[-1]:.3e}")
+    return np.array(hist)
 
 
 class Extrapolator:
@@ -240,11 +312,26 @@ class Extrapolator:
         self.mlp.set_norm(self.K, self.M, self.F, self.norm[0], self.norm[1], self.norm[2], self.norm[3])
 
     def train(self, feat, steps, batch=512, lr=1e-3, lr_min=1e-5, weight_decay=0.0, t_min=0, seed=0, log=None,
-              pushforward=0, noise=0.0, warm=0.25):
+              pushforward=0, noise=0.0, warm=0.25, pg=None):
         """Adam on random windows (cosine learning-rate decay); after the first
         `warm` fraction of the steps, each step first rolls the network forward
         r ~ U{0..pushforward} blocks and trains on the windows it produced.
-        Returns the loss history (one value per step)."""
+        With a process group ``pg`` every rank holds its own trajectories and
+        the training is data-parallel (train_data_parallel; the normalisation
+        is rank 0's).  Returns the loss history (one value per step)."""
+        if pg is not None:
+            if pushforward or noise:
+                raise ValueError("data-parallel training covers plain windows (no pushforward, no noise)")
+            torch = _torch()
+            if self.norm is None:
+                self.fit_norm(feat, t_min)
+            v = torch.as_tensor(np.concatenate([self.norm[0], np.array(self.norm[1:], np.float32)]),
+                                device=feat.device)
+            v = broadcast_from_root(v, pg).cpu().numpy()
+            self.norm = (v[:-3], float(v[-3]), float(v[-2]), float(v[-1]))
+            self.mlp.set_norm(self.K, self.M, self.F, self.norm[0], self.norm[1], self.norm[2], self.norm[3])
+            return train_data_parallel(self.mlp, feat, steps, max(self.K - 1, t_min), feat.shape[1] - self.M, pg,
+                                       batch, lr, lr_min, weight_decay, seed, log)
         if self.norm is None:
             self.fit_norm(feat, t_min)
         rng = np.random.default_rng(seed)

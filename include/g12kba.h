@@ -254,6 +254,14 @@ int g12_mlp_windows(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t sn
                     int32_t batch, float *X_dev, float *Y_dev);
 int g12_mlp_train_windows(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t snaps, const int64_t *idx,
                           int32_t batch, float lr, float weight_decay, double *loss);
+/* windows, loss and gradients of one batch without the Adam step (returns
+ * once the gradients are complete on the device) */
+int g12_mlp_grad_windows(g12_mlp *m, const float *feat_dev, int32_t ntraj, int64_t snaps, const int64_t *idx,
+                         int32_t batch, double *loss);
+/* the device block holding every weight and bias gradient (segments padded to
+ * 64 floats, padding zero): data-parallel training reduces it across ranks
+ * between g12_mlp_grad_windows and g12_mlp_adam */
+int g12_mlp_grad_buffer(g12_mlp *m, float **grads_dev, int64_t *count);
 /* one step after r blocks of the network's own rollout from windows ending at
  * idx's t (targets: the true snapshots that follow); noise: Gaussian input
  * noise in normalised units (0: none) */

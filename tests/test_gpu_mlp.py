@@ -133,3 +133,77 @@ def test_batch_features_match_context_trajectory(g12, torch, learned):
         want = learned.features(np.concatenate([traj[4::4], st[0][None]], axis=0))
         assert np.allclose(feat[i], want[: feat.shape[1]], rtol=0, atol=1e-6)
         assert np.allclose(dip[i], g12.dipole(traj), atol=1e-12)
+
+
+def test_gradient_block_and_split_step(torch, learned):
+    """The data-parallel pieces: grad_windows + adam is the fused training step
+    (up to summation order: the split-K GEMMs accumulate with atomics), and the
+    gradient block's view holds every gradient (segments padded to 64 floats)."""
+    n, K, M = 15, 8, 8
+    F = n * (n + 1)
+    dims = (K * F, 128, 128, 128, M * F)
+    rng = np.random.default_rng(11)
+    feat = torch.from_numpy((0.3 * rng.standard_normal((4, 80, F))).astype(np.float32)).cuda()
+    mean = feat.mean(dim=(0, 1)).cpu().numpy()
+    idx = np.stack([rng.integers(0, 4, 128), rng.integers(K - 1, 80 - M, 128)], axis=1)
+    with learned.MLP(dims, max_batch=128, seed=5) as a, learned.MLP(dims, max_batch=128, seed=5) as b:
+        for net in (a, b):
+            net.set_norm(K, M, F, mean, 0.5, 0.7, 0.2)
+        p0 = a.get_params()
+        la = a.train_windows(feat, idx, 1e-3)
+        lb = b.grad_windows(feat, idx)
+        g_host = b.grads()
+        g_view = b.grad_tensor().cpu().numpy()
+        b.adam(1e-3)
+        # a sum that lands on the other side of a bf16 rounding boundary moves the
+        # next layer's operand by 2^-8, so agreement is to the oracle bar
+        assert abs(la - lb) <= GRAD_TOL * abs(la), (la, lb)
+        ge = _relf(g_host, a.grads())
+        assert ge <= GRAD_TOL, ge
+        da, db = a.get_params() - p0, b.get_params() - p0
+        assert _relf(db, da) <= 1e-2, _relf(db, da)
+    off, parts = 0, []
+    for l in range(4):
+        for cnt in (dims[l] * dims[l + 1], dims[l + 1]):
+            parts.append(g_view[off:off + cnt])
+            assert not np.any(g_view[off + cnt:off + (cnt + 63) // 64 * 64])
+            off += (cnt + 63) // 64 * 64
+    assert off == g_view.size
+    assert np.array_equal(np.concatenate(parts), g_host)
+
+
+def test_data_parallel_one_rank_matches_fused_steps(torch, learned):
+    """With one rank the data-parallel loop takes the fused training steps on
+    the same windows (up to summation order)."""
+    import os
+    import socket
+
+    import torch.distributed as dist
+    n, K, M = 15, 8, 8
+    F = n * (n + 1)
+    dims = (K * F, 128, 128, 128, M * F)
+    rng = np.random.default_rng(12)
+    feat = torch.from_numpy((0.3 * rng.standard_normal((4, 80, F))).astype(np.float32)).cuda()
+    mean = feat.mean(dim=(0, 1)).cpu().numpy()
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        with learned.MLP(dims, max_batch=128, seed=6) as a, learned.MLP(dims, max_batch=128, seed=6) as b:
+            for net in (a, b):
+                net.set_norm(K, M, F, mean, 0.5, 0.7, 0.2)
+            ha = learned.train_data_parallel(a, feat, 5, K - 1, 80 - M, None, 128, 1e-3, 1e-3, seed=4)
+            r = np.random.default_rng([4, 0])
+            hb = []
+            for _ in range(5):
+                idx = np.stack([r.integers(0, 4, 128), r.integers(K - 1, 80 - M, 128)], axis=1)
+                hb.append(b.train_windows(feat, idx, 1e-3))
+            assert np.allclose(ha, np.array(hb), rtol=GRAD_TOL, atol=0), (ha, hb)
+            p0 = learned.MLP(dims, max_batch=128, seed=6)
+            q0 = p0.get_params()
+            p0.close()
+            assert _relf(a.get_params() - q0, b.get_params() - q0) <= 1e-2
+    finally:
+        dist.destroy_process_group()
