@@ -155,3 +155,16 @@ def test_total_energy_oracle_steps(oracle):
     E = total_energy(oracle, cfg, G1, XX, XY)
     assert abs(E[0] - E0[0]) <= 1e-11 * abs(E0[0])
     assert abs(E[3] - E0[3]) > 1e-3
+
+
+def test_hf_energy_conserved_by_reference_run(oracle):
+    """HF-only propagation (G2 frozen at zero): the one-body plus Hartree-Fock
+    energy is constant along the reference's own trajectory (31 snapshots of
+    tests/golden/run_hf.npz)."""
+    from oracle import total_energy
+    g = load_golden("run_hf.npz")
+    cfg = Config(**{k[4:]: g[k].item() for k in g.files if k.startswith("cfg_")})
+    zero = np.zeros(cfg.n ** 4, np.complex128)
+    E = np.array([total_energy(oracle, cfg, G1, zero, zero)[0] for G1 in g["traj_every10"]])
+    assert np.ptp(E) <= 1e-11 * abs(E[0])
+    assert abs(total_energy(oracle, cfg, g["g1_as"], zero, zero)[0] - E[0]) <= 1e-11 * abs(E[0])
