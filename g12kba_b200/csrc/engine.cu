@@ -57,6 +57,7 @@ struct g12_ctx {
     void *evict_buf = nullptr;      // g12_set_l2_eviction: written after every step
     size_t evict_bytes = 0;
     double *energy_dev = nullptr;   // g12_total_energy result (4 doubles)
+    std::vector<cudaEvent_t> ring;  // per-step event pairs of the eviction timing
 };
 
 namespace {
@@ -285,17 +286,35 @@ int run_steps(g12_ctx *ctx, long long steps, double *traj_out, double *dip_out, 
         const int G = ctx->lc.steps_per_graph;
         if (ctx->evict_bytes) {
             // L2 eviction between timed graph launches: each launch is timed on
-            // its own and the eviction write follows its end event
-            for (long long q = 0; q < chunk; q += G) {
-                CK(cudaEventRecord(ctx->ev0, ctx->s));
-                CK(cudaGraphLaunch(ctx->graph, ctx->s));
-                CK(cudaEventRecord(ctx->ev1, ctx->s));
-                CK(cudaMemsetAsync(ctx->evict_buf, 0, ctx->evict_bytes, ctx->s));
-                CK(cudaEventSynchronize(ctx->ev1));
-                float ms = 0;
-                cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-                total_ms += ms;
+            // its own (an event pair around it) and the eviction write follows
+            // its end event.  The launches are queued ahead of the device (a ring
+            // of event pairs, read back every kRing launches), so no host
+            // submission gap falls inside a timed span.
+            constexpr int kRing = 32;
+            if (ctx->ring.empty()) {
+                ctx->ring.resize(2 * kRing);
+                for (auto &e : ctx->ring) CK(cudaEventCreate(&e));
             }
+            int used = 0;
+            auto drain = [&]() -> bool {
+                if (!used) return true;
+                if (!ck(ctx, cudaEventSynchronize(ctx->ring[2 * used - 1]), "cudaEventSynchronize")) return false;
+                for (int j = 0; j < used; ++j) {
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, ctx->ring[2 * j], ctx->ring[2 * j + 1]);
+                    total_ms += ms;
+                }
+                used = 0;
+                return true;
+            };
+            for (long long q = 0; q < chunk; q += G) {
+                CK(cudaEventRecord(ctx->ring[2 * used], ctx->s));
+                CK(cudaGraphLaunch(ctx->graph, ctx->s));
+                CK(cudaEventRecord(ctx->ring[2 * used + 1], ctx->s));
+                CK(cudaMemsetAsync(ctx->evict_buf, 0, ctx->evict_bytes, ctx->s));
+                if (++used == kRing && !drain()) return G12_ERR_CUDA;
+            }
+            if (!drain()) return G12_ERR_CUDA;
         } else {
             CK(cudaEventRecord(ctx->ev0, ctx->s));
             for (long long q = 0; q < chunk; q += G) CK(cudaGraphLaunch(ctx->graph, ctx->s));
@@ -465,6 +484,7 @@ extern "C" int g12_destroy(g12_ctx *ctx)
     if (ctx->sched_host) cudaFreeHost(ctx->sched_host);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    for (cudaEvent_t e : ctx->ring) cudaEventDestroy(e);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     if (ctx->s2) cudaStreamDestroy(ctx->s2);
