@@ -453,7 +453,7 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     lc.prep_smem = prep_smem();
     lc.g1_blocks = g1_blocks(n2);
     lc.g1_smem = g1_smem(n2);
-    lc.steps_per_graph = n <= 8 ? 8 : (n <= 16 ? 4 : 1);
+    lc.steps_per_graph = n <= 8 ? 8 : (n <= 32 ? 4 : 1);
     if (!ck(ctx, cudaFuncSetAttribute(k_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.ab_smem)), "attr") ||
         !ck(ctx, cudaFuncSetAttribute(k_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.cd_smem)), "attr") ||
         !ck(ctx, cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.prep_smem)), "attr") ||
@@ -702,7 +702,7 @@ extern "C" int32_t g12_set_l2_eviction(g12_ctx *ctx, int64_t bytes)
     if (ctx->evict_buf) cudaFree(ctx->evict_buf);
     ctx->evict_buf = nullptr;
     ctx->evict_bytes = 0;
-    ctx->lc.steps_per_graph = ctx->n <= 8 ? 8 : (ctx->n <= 16 ? 4 : 1);
+    ctx->lc.steps_per_graph = ctx->n <= 8 ? 8 : (ctx->n <= 32 ? 4 : 1);
     if (bytes == 0) return G12_OK;
     if (cudaMalloc(&ctx->evict_buf, size_t(bytes)) != cudaSuccess) {
         cudaGetLastError();
