@@ -20,7 +20,9 @@
 //     other host threads) race on it and must be serialised by the caller.
 //   - The first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) and sets kernel attributes; make that first call
-//     before any stream capture.
+//     before any stream capture.  That set-up is cached per device ordinal for
+//     the life of the process and does not survive cudaDeviceReset: do not
+//     call this entry point after resetting a device it was used on.
 #include "g12kba.h"
 #include "internal.h"
 
@@ -140,13 +142,26 @@ extern "C" int g12_rhs_noalloc(const g12_params *p, const double *G1_dev, const 
         return G12_ERR_INVALID;
     }
     const int Ns = p->Ns, Nb = p->Nb, n = Ns * Nb;
-    if (Ns < 1 || Nb < 1 || n > kMax) {
+    if (Ns < 1 || Nb < 1) {
+        set_err(err, errcap, "g12_rhs_noalloc: invalid Ns = " + std::to_string(Ns) + ", Nb = " + std::to_string(Nb) +
+                                 " (both must be >= 1)");
+        return G12_ERR_INVALID;
+    }
+    if (n > kMax) {
         set_err(err, errcap, "g12_rhs_noalloc: n = Ns*Nb = " + std::to_string(n) +
                                  " exceeds the static scratch limit G12_NOALLOC_MAX_N = " + std::to_string(kMax));
         return G12_ERR_INVALID;
     }
+    // an error left pending by earlier, unrelated work of the caller is reported
+    // as such (and cleared), not blamed on this call's launches
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_err(err, errcap, std::string("g12_rhs_noalloc: a CUDA error from earlier work was pending on entry "
+                                         "(nothing was launched): ") + cudaGetErrorString(e));
+        return G12_ERR_CUDA;
+    }
     int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    e = cudaGetDevice(&dev);
     if (e != cudaSuccess) {
         set_err(err, errcap, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
         return G12_ERR_NO_DEVICE;
@@ -232,8 +247,12 @@ extern "C" int g12_rhs_noalloc(const g12_params *p, const double *G1_dev, const 
         K::k_to_ref<<<64, 256, 0, s>>>(d.TMP0 + n4, reinterpret_cast<double2 *>(K2xy_dev), Ns, Nb, n4);
     } else {
         // no two-body terms (RK_solver.h:154): K2 is zero
-        cudaMemsetAsync(K2xx_dev, 0, size_t(n4) * sizeof(double2), s);
-        cudaMemsetAsync(K2xy_dev, 0, size_t(n4) * sizeof(double2), s);
+        if ((e = cudaMemsetAsync(K2xx_dev, 0, size_t(n4) * sizeof(double2), s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(K2xy_dev, 0, size_t(n4) * sizeof(double2), s)) != cudaSuccess) {
+            cudaGetLastError();
+            set_err(err, errcap, std::string("g12_rhs_noalloc: cudaMemsetAsync of K2: ") + cudaGetErrorString(e));
+            return G12_ERR_CUDA;
+        }
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) {

@@ -215,7 +215,9 @@ int32_t g12_batch_tile(const g12_batch *b, int32_t i);  /* autotuned matrices pe
  * in `err`).  Calls share that array: calls whose GPU work overlaps race and
  * must be serialised by the caller.  The first call on a device performs a
  * one-time set-up (symbol address lookup, kernel attributes) and should come
- * before any stream capture. */
+ * before any stream capture; that set-up is kept per device ordinal and does
+ * not survive cudaDeviceReset.  A CUDA error left pending by earlier work is
+ * reported as such (G12_ERR_CUDA, nothing launched). */
 #define G12_NOALLOC_MAX_N 16
 int g12_rhs_noalloc(const g12_params *p, const double *G1_dev, const double *G2xx_dev,
                     const double *G2xy_dev, double U_eff, double w_quench, int32_t Nq_eff,

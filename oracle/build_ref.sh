@@ -19,7 +19,11 @@ REFROOT="${G12_REFERENCE:-/root/reference}"
 HDR="$REFROOT/G12KBA-GW/src/headers"
 OUT="$HERE/_ref"
 if [ ! -d "$HDR" ]; then
-    echo "build_ref: reference headers not found at $HDR" >&2
+    if [ "${1:-}" = "--if-present" ]; then
+        echo "build_ref: no reference checkout at $REFROOT (set G12_REFERENCE); oracle/_ref not rebuilt"
+        exit 0
+    fi
+    echo "build_ref: reference headers not found at $HDR (set G12_REFERENCE)" >&2
     exit 1
 fi
 mkdir -p "$OUT"

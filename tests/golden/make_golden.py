@@ -137,7 +137,10 @@ def energy_pin():
 def sample_input():
     """The reference's only fixture (G12KBA-GW/input), kept verbatim as test
     data for the input reader."""
-    src = os.path.join(os.environ.get("G12_REFERENCE", "/root/reference"), "G12KBA-GW", "input")
+    root = os.environ.get("G12_REFERENCE")
+    if not root:
+        sys.exit("set G12_REFERENCE to the reference checkout (the directory holding G12KBA-GW/)")
+    src = os.path.join(root, "G12KBA-GW", "input")
     with open(src, "rb") as f, open(os.path.join(OUT, "sample_input"), "wb") as g:
         g.write(f.read())
 
