@@ -276,6 +276,28 @@ def extended_model_measure(g12, local):
     return out
 
 
+def full_run_error(g12, p, S, precision, local):
+    """The workload's full run (10,000 RK4 steps from the post-switching state
+    S) on `precision` and on plain FP64; max G1 and dipole errors of the
+    trajectory (error definitions of the tests: G1 relative to max |G1|,
+    dipole relative to max |p|)."""
+    T = g12.rk_iterations(p)
+    out = {"iterations": T}
+    trajs = {}
+    for prec in ("fp64", precision):
+        with g12.Context(p, prec, local) as ctx:
+            ctx.set_state(*S)
+            tr, rc = ctx.propagate(T)
+            out[prec + "_status"] = rc
+            out[prec + "_device_s"] = ctx.last_device_ms / 1e3
+        trajs[prec] = tr
+    ref, got = trajs["fp64"], trajs[precision]
+    out["g1_max_rel_err"] = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+    pr, pg_ = g12.dipole(ref), g12.dipole(got)
+    out["dipole_max_rel_err"] = float(np.max(np.abs(pg_ - pr)) / max(np.max(np.abs(pr)), 1e-12))
+    return out
+
+
 def learned_measure(g12, local, ntrain=128, ntest=32, T=3000, P=150, train_steps=20000, check_every=200):
     """Learned extrapolator on its n=16 family (Ns=8, Nb=2, U ~ U[1,3],
     quench ~ U[0.5,3] switched on at t=1): trajectories from the batch engine,
@@ -377,6 +399,7 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-extended", action="store_true")
+    ap.add_argument("--no-full-run", action="store_true")
     ap.add_argument("--skip-as", action="store_true",
                     help="start the timed steps from G0 (profiling runs); the cost of a step does not depend on the state")
     args = ap.parse_args()
@@ -485,17 +508,44 @@ def main():
         mx.close()
     fp.close()
 
-    ensemble = None
+    # the same timed steps on the FP64 symmetric engine (one contraction per
+    # tensor and the compressed state, all in FP64): splits the mixed engine's
+    # speed-up into its symmetry part and its precision part
+    fp64sym = None
+    if mixed and p.n in (8, 16, 32):
+        with g12.Context(p, "fp64sym", local) as sy:
+            sy.set_state(*S)
+            sy.propagate_dipole(args.warmup)
+            sy.set_l2_eviction(EVICT_BYTES)
+            barrier(pg)
+            sy.set_state(*S)
+            traj_sy, rc_sy = sy.propagate(K)
+            ms_sy = allmax(pg, sy.last_device_ms)
+        fp64sym = {"value": world * K / (ms_sy / 1e3), "unit": "steps/s", "ms_per_step": ms_sy / K,
+                   "status": rc_sy, "g1_max_rel_err_vs_fp64": float(np.max(np.abs(traj_sy - traj_fp)) /
+                                                                    np.max(np.abs(traj_fp)))}
+
+    # error of the full 10,000-step run of the workload (untimed): this engine
+    # against plain FP64 from the same post-switching state
+    full_run = None
+    if mixed and rank == 0 and not args.no_full_run:
+        full_run = full_run_error(g12, p, S, args.precision, local)
+
+    sections = []
+
+    def section(name, obj):
+        # the large sub-results go on their own lines before the headline line
+        if rank == 0 and obj is not None:
+            print(json.dumps({"section": name, name: obj}), flush=True)
+            sections.append(name)
+
+    section("full_run", full_run)
     if not args.no_ensemble:
-        ensemble = ensemble_measure(g12, local, rank, world, pg)
-
-    extended = None
+        section("ensemble", ensemble_measure(g12, local, rank, world, pg))
     if rank == 0 and not args.no_extended:
-        extended = extended_model_measure(g12, local)
-
-    learned = None
+        section("extended_model_n16", extended_model_measure(g12, local))
     if rank == 0 and not args.no_learned:
-        learned = learned_measure(g12, local)
+        section("learned", learned_measure(g12, local))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -517,13 +567,17 @@ def main():
                                          "status": rc_fp},
             "speedup_vs_plain_fp64": value / value_fp,
             "g1_max_rel_err_vs_fp64": g1_err,
+            "fp64_symmetric": fp64sym,
+            "full_run_err_vs_fp64": None if full_run is None else {
+                k: full_run[k] for k in ("iterations", "g1_max_rel_err", "dipole_max_rel_err")},
             "energy": {"start": float(E_start[0]), "correlation_start": float(E_start[3]),
                        "fp64_rel_drift": float(abs(E_fp[0] - E_start[0]) / abs(E_start[0])),
                        "mixed_rel_drift": float(abs(E_mx[0] - E_start[0]) / abs(E_start[0])),
                        "correlation_change": float(E_mx[3] - E_start[3]),
                        "note": "g12_total_energy before and after the timed steps (constant U, quench masked)"},
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline,
-            "kernels": kernels, "ensemble": ensemble, "extended_model_n16": extended, "learned": learned, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "kernels": kernels, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "sections_printed_above": sections,
         }
         print(json.dumps(line))
     if pg is not None:

@@ -23,7 +23,7 @@ HEADER = os.path.join(os.path.dirname(PKG), "include", "g12kba.h")
 
 G12_OK = 0
 G12_GUARD_TRIPPED = 1
-PREC = {"fp64": 0, "tf32x3": 1, "bf16oz": 2, "fp32": 3, "tf32x6": 4}
+PREC = {"fp64": 0, "tf32x3": 1, "bf16oz": 2, "fp32": 3, "tf32x6": 4, "fp64sym": 5}
 QUENCH = {"full": 0, "pulse": 1}
 VLAW = {"exp": 0, "inv": 1}
 

@@ -369,7 +369,7 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
         g_create_error = "unsupported size: need 1 <= Ns*Nb <= 64";
         return G12_ERR_INVALID;
     }
-    if (precision < G12_PREC_FP64 || precision > G12_PREC_TF32X6) {
+    if (precision < G12_PREC_FP64 || precision > G12_PREC_FP64SYM) {
         g_create_error = "unknown precision mode";
         return G12_ERR_INVALID;
     }

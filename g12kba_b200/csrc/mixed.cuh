@@ -25,6 +25,7 @@ struct MixedState {
     bool tc = false;  // tensor-core contraction (else FP32 SIMT)
     int pieces = 2;   // tf32 pieces per operand (2: 3 products, 3: 6 products)
     bool oz = false;  // exact integer-digit bf16 products
+    bool dbl = false; // FP64SYM: FP64 stage input and W, FP64 SIMT contraction
     SymDev s{};
     CUtensorMap map_a{}, map_b{};  // TMA views of TMPa / TMPb
     unsigned char *ozb = nullptr;  // h digit tiles (written by k_prep, read by k_sym_gemm_oz2)
@@ -44,6 +45,11 @@ inline bool mixed_supported(int n, int prec, std::string *why)
     if (prec == 3) {
         if (n == 8 || n == 16 || n == 32 || n == 64) return true;
         if (why) *why = "the FP32 symmetric engine needs n = Ns*Nb in {8, 16, 32, 64}";
+        return false;
+    }
+    if (prec == 5) {
+        if (n == 8 || n == 16 || n == 32) return true;
+        if (why) *why = "the FP64 symmetric engine needs n = Ns*Nb in {8, 16, 32}";
         return false;
     }
     return false;
@@ -89,7 +95,8 @@ inline bool encode_tmp_map(CUtensorMap *map, float *base, int n, std::string *er
     return true;
 }
 
-// prec: 1 = TF32X3, 4 = TF32X6, 2 = BF16 exact digits (tcgen05), 3 = FP32 SIMT.
+// prec: 1 = TF32X3, 4 = TF32X6, 2 = BF16 exact digits (tcgen05), 3 = FP32 SIMT,
+// 5 = FP64 SIMT (FP64 stage input and W).
 inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
 {
     const int n = d.n;
@@ -97,6 +104,8 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
     m.prec = prec;
     m.tc = (prec == 1 || prec == 2 || prec == 4);
     m.oz = (prec == 2);
+    m.dbl = (prec == 5);
+    const size_t ts = m.dbl ? 2 : 1;  // floats per stored TMP / W value
     m.pieces = (prec == 4) ? 3 : 2;
     SymDev &s = m.s;
     s.d = d;
@@ -129,8 +138,8 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
         for (int b = a; b < s.nblk; ++b) pairs.push_back(make_int2(a, b));
     int *gc = nullptr, *gp = nullptr;
     int2 *pp = nullptr;
-    bool ok = mixed_alloc(m, &s.TMPa, size_t(2 * 2 * n4)) && mixed_alloc(m, &s.TMPb, size_t(2 * 2 * n4)) &&
-              mixed_alloc(m, &s.W, size_t(2 * 2 * n4)) && mixed_alloc(m, &s.Yc, size_t(2) * s.npairs * kTB * kTB) &&
+    bool ok = mixed_alloc(m, &s.TMPa, ts * size_t(2 * 2 * n4)) && mixed_alloc(m, &s.TMPb, ts * size_t(2 * 2 * n4)) &&
+              mixed_alloc(m, &s.W, ts * size_t(2 * 2 * n4)) && mixed_alloc(m, &s.Yc, size_t(2) * s.npairs * kTB * kTB) &&
               mixed_alloc(m, &s.Ac, size_t(2) * s.npairs * kTB * kTB) && mixed_alloc(m, &s.Qt, size_t(2 * n3)) &&
               mixed_alloc(m, &s.Rtt, size_t(n2 * d.Ns)) && mixed_alloc(m, &gc, cs.size()) &&
               mixed_alloc(m, &gp, cs.size()) && mixed_alloc(m, &pp, pairs.size()) && mixed_alloc(m, &s.err, 1);
@@ -144,14 +153,22 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
     s.gemm_c = gc;
     s.gemm_partner = gp;
     s.pairs = pp;
-    m.epi_smem = size_t(n) * (n + 1) * sizeof(double2) + 2 * kTB * (kTB + 1) * sizeof(float2) + kTB * (kTB + 1) * sizeof(double2);
+    m.epi_smem = size_t(n) * (n + 1) * sizeof(double2) + 2 * kTB * (kTB + 1) * ts * sizeof(float2) +
+                 kTB * (kTB + 1) * sizeof(double2);
     m.epi_smem = std::max(m.epi_smem, g1_smem(n2));  // G1-side blocks of k_sym_epi
-    m.simt_smem = (size_t(128) * 2 * n + size_t(128) * (2 * n + 1)) * sizeof(float) + size_t(n2) * sizeof(float2);
-    cudaFuncSetAttribute(k_sym_epi<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
-    cudaFuncSetAttribute(k_sym_epi<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
-    cudaFuncSetAttribute(k_sym_epi<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
-    cudaFuncSetAttribute(k_sym_epi<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
-    cudaFuncSetAttribute(k_sym_gemm_simt, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.simt_smem));
+    m.simt_smem = ts * ((size_t(128) * 2 * n + size_t(128) * (2 * n + 1)) * sizeof(float) + size_t(n2) * sizeof(float2));
+    if (m.dbl) {
+        cudaFuncSetAttribute(k_sym_epi<8, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+        cudaFuncSetAttribute(k_sym_epi<16, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+        cudaFuncSetAttribute(k_sym_epi<32, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+        cudaFuncSetAttribute(k_sym_gemm_simt<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.simt_smem));
+    } else {
+        cudaFuncSetAttribute(k_sym_epi<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+        cudaFuncSetAttribute(k_sym_epi<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+        cudaFuncSetAttribute(k_sym_epi<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+        cudaFuncSetAttribute(k_sym_epi<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
+        cudaFuncSetAttribute(k_sym_gemm_simt<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.simt_smem));
+    }
     if (m.tc) {
         if (!encode_tmp_map(&m.map_a, s.TMPa, n, err) || !encode_tmp_map(&m.map_b, s.TMPb, n, err)) return -2;
         int sms = 148;
@@ -201,7 +218,8 @@ inline void mixed_free(MixedState &m)
 inline int mixed_on_state(MixedState &m, const Dev &d, cudaStream_t st)
 {
     m.s.d = d;
-    k_sym_pack<<<dim3(m.s.npairs, 2), 256, 0, st>>>(m.s, d.Y2);
+    if (m.dbl) k_sym_pack<double><<<dim3(m.s.npairs, 2), 256, 0, st>>>(m.s, d.Y2);
+    else k_sym_pack<float><<<dim3(m.s.npairs, 2), 256, 0, st>>>(m.s, d.Y2);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
@@ -217,7 +235,7 @@ inline int mixed_kernel_kinds(const MixedState &) { return 2; }
 
 inline const char *mixed_kernel_name(const MixedState &m, int q)
 {
-    if (q == 0) return m.oz2 ? "k_sym_gemm_oz2" : (m.tc ? "k_sym_gemm_tc" : "k_sym_gemm_simt");
+    if (q == 0) return m.oz2 ? "k_sym_gemm_oz2" : (m.tc ? "k_sym_gemm_tc" : (m.dbl ? "k_sym_gemm_simt<f64>" : "k_sym_gemm_simt"));
     if (q == 1) return "k_sym_epi";
     return "";
 }
@@ -261,8 +279,10 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
             else if (s.n == 32) k_sym_gemm_tc<32, 3><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else if (m.pieces == 2) k_sym_gemm_tc<16, 2><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
             else k_sym_gemm_tc<16, 3><<<m.tc_grid, 128, m.tc_smem, st>>>(s, k, map);
+        } else if (m.dbl) {
+            k_sym_gemm_simt<double><<<2 * s.gemm_tiles, 256, m.simt_smem, st>>>(s, k);
         } else {
-            k_sym_gemm_simt<<<2 * s.gemm_tiles, 256, m.simt_smem, st>>>(s, k);
+            k_sym_gemm_simt<float><<<2 * s.gemm_tiles, 256, m.simt_smem, st>>>(s, k);
         }
     } else {
         const dim3 g(s.npairs, 2);
@@ -272,6 +292,12 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
             const dim3 gf(s.npairs + sf.g1x, 2);
             if (s.n == 32) launch_pdl(k_sym_epi<32>, gf, dim3(256), m.epi_smem, st, sf, k);
             else launch_pdl(k_sym_epi<16>, gf, dim3(256), m.epi_smem, st, sf, k);
+            return;
+        }
+        if (m.dbl) {
+            if (s.n == 32) k_sym_epi<32, double><<<g, 256, m.epi_smem, st>>>(s, k);
+            else if (s.n == 16) k_sym_epi<16, double><<<g, 256, m.epi_smem, st>>>(s, k);
+            else k_sym_epi<8, double><<<g, 256, m.epi_smem, st>>>(s, k);
             return;
         }
         if (s.n == 32 && m.oz2) launch_pdl(k_sym_epi<32>, g, dim3(256), m.epi_smem, st, s, k);

@@ -13,9 +13,9 @@
 // e), k_sym_epi forms C = W - W^H on pairs of 32 x 32 tiles (R, C) / (C, R) and
 // fuses the rest of the stage (Psi, Pi, K2, RK4 bookkeeping) like k_apply<true>.
 //
-// Storage (per tensor t = xx, xy):
-//   TMP  (FP32, GEMM input):  ((mu2*n^2 + c)*2 + part)*n + mu1
-//   W    (FP32):              (c*2 + part)*n^2 + r
+// Storage (per tensor t = xx, xy; TT = FP32 in the mixed modes, FP64 in FP64SYM):
+//   TMP  (TT, GEMM input):    ((mu2*n^2 + c)*2 + part)*n + mu1
+//   W    (TT):                (c*2 + part)*n^2 + r
 //   Yc, Ac (FP64 complex):    Hermitian-compressed state and RK4 sum: for each
 //                             tile pair p = (Rb <= Cb) of 32 x 32 blocks,
 //                             [p][c_local*32 + r_local].
@@ -54,29 +54,54 @@ __device__ __forceinline__ void l2_prefetch_bulk(const void *p, unsigned bytes)
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// stage k reads TMPb (k even) or TMPa (k odd) and writes the other one
-__device__ __forceinline__ const float *sym_in(const SymDev &s, int k) { return (k & 1) ? s.TMPa : s.TMPb; }
-__device__ __forceinline__ float *sym_out(const SymDev &s, int k) { return (k & 1) ? s.TMPb : s.TMPa; }
+// stage k reads TMPb (k even) or TMPa (k odd) and writes the other one.  TT is
+// the storage type of TMP and W: float (mixed modes) or double (FP64SYM).
+template <typename TT = float>
+__device__ __forceinline__ const TT *sym_in(const SymDev &s, int k)
+{
+    return reinterpret_cast<const TT *>((k & 1) ? s.TMPa : s.TMPb);
+}
+template <typename TT = float>
+__device__ __forceinline__ TT *sym_out(const SymDev &s, int k)
+{
+    return reinterpret_cast<TT *>((k & 1) ? s.TMPb : s.TMPa);
+}
+
+// complex pair of the storage type
+template <typename TT> struct Cx2;
+template <> struct Cx2<float> { using T = float2; };
+template <> struct Cx2<double> { using T = double2; };
+template <typename TT>
+__device__ __forceinline__ typename Cx2<TT>::T mk2(TT a, TT b)
+{
+    typename Cx2<TT>::T v;
+    v.x = a;
+    v.y = b;
+    return v;
+}
 
 __device__ __forceinline__ long long tmp_index(int n, int mu1, int mu2, int c, int part)
 {
     return (((long long)mu2 * n * n + c) * 2 + part) * n + mu1;
 }
 
-// Reference FP32 SIMT version of the W contraction (same tiles as the
-// tensor-core kernel): T1[mu1][mu2][c] = sum_rho h[mu1][rho] X[rho][mu2][c].
+// SIMT version of the W contraction in the storage type TT (FP32: the checker
+// of the tensor-core kernels; FP64: the FP64SYM engine), same tiles as the
+// tensor-core kernel: T1[mu1][mu2][c] = sum_rho h[mu1][rho] X[rho][mu2][c].
+template <typename TT>
 __global__ void __launch_bounds__(256) k_sym_gemm_simt(SymDev s, int k)
 {
     if (!*s.d.active) return;
+    using T2 = typename Cx2<TT>::T;
     const int n = s.n, cpt = s.cpt, rows = cpt * n;
-    extern __shared__ float smf[];
-    float *X = smf;                         // [rows][2n]
-    float *S = X + rows * 2 * n;            // [rows][2n + 1] (T1 staging)
-    float2 *H = reinterpret_cast<float2 *>(S + rows * (2 * n + 1));  // [n][n]
+    extern __shared__ double smsimt[];
+    TT *X = reinterpret_cast<TT *>(smsimt);  // [rows][2n]
+    TT *S = X + rows * 2 * n;                // [rows][2n + 1] (T1 staging)
+    T2 *H = reinterpret_cast<T2 *>(S + rows * (2 * n + 1));  // [n][n] (rows = 128: 16-byte aligned)
     const int t = blockIdx.x / s.gemm_tiles, g = blockIdx.x % s.gemm_tiles;
-    const float *Xg = sym_in(s, k) + t * 2 * s.n4;
+    const TT *Xg = sym_in<TT>(s, k) + t * 2 * s.n4;
     for (int x = threadIdx.x; x < n * n; x += blockDim.x)
-        H[x] = make_float2(float(s.d.h[x].x), float(s.d.h[x].y));
+        H[x] = mk2<TT>(TT(s.d.h[x].x), TT(s.d.h[x].y));
     for (int e = threadIdx.x; e < rows * 2 * n; e += blockDim.x) {
         const int row = e / (2 * n), kk = e % (2 * n);
         const int slot = row / n, mu2 = row % n;
@@ -86,28 +111,28 @@ __global__ void __launch_bounds__(256) k_sym_gemm_simt(SymDev s, int k)
     __syncthreads();
     for (int e = threadIdx.x; e < rows * n; e += blockDim.x) {
         const int row = e / n, mu1 = e % n;
-        float re = 0.f, im = 0.f;
-        const float *xr = X + row * 2 * n;
+        TT re = 0, im = 0;
+        const TT *xr = X + row * 2 * n;
         for (int r = 0; r < n; ++r) {
-            const float2 hv = H[mu1 * n + r];
-            const float gr = xr[r], gi = xr[n + r];
-            re = fmaf(hv.x, gr, re);
-            re = fmaf(-hv.y, gi, re);
-            im = fmaf(hv.x, gi, im);
-            im = fmaf(hv.y, gr, im);
+            const T2 hv = H[mu1 * n + r];
+            const TT gr = xr[r], gi = xr[n + r];
+            re = fma(hv.x, gr, re);
+            re = fma(-hv.y, gi, re);
+            im = fma(hv.x, gi, im);
+            im = fma(hv.y, gr, im);
         }
         S[row * (2 * n + 1) + mu1] = re;
         S[row * (2 * n + 1) + n + mu1] = im;
     }
     __syncthreads();
     // W[mu1][mu2][c] = T1[mu1][mu2][c] + T1[mu2][mu1][cbar]
-    float *Wg = s.W + t * 2 * s.n4;
+    TT *Wg = reinterpret_cast<TT *>(s.W) + t * 2 * s.n4;
     const long long n2 = (long long)n * n;
     for (int e = threadIdx.x; e < cpt * 2 * n * n; e += blockDim.x) {
         const int r = e % (n * n), part = (e / (n * n)) % 2, slot = e / (2 * n * n);
         const int mu1 = r % n, mu2 = r / n;
         const int ps = s.gemm_partner[g * cpt + slot];
-        const float v = S[(slot * n + mu2) * (2 * n + 1) + part * n + mu1] +
+        const TT v = S[(slot * n + mu2) * (2 * n + 1) + part * n + mu1] +
                         S[(ps * n + mu1) * (2 * n + 1) + part * n + mu2];
         const int c = s.gemm_c[g * cpt + slot];
         Wg[((long long)c * 2 + part) * n2 + r] = v;
@@ -115,11 +140,12 @@ __global__ void __launch_bounds__(256) k_sym_gemm_simt(SymDev s, int k)
 }
 
 // Stage epilogue on a tile pair (R, C) / (C, R): C = W - W^H, Psi, Pi, K2,
-// RK4 bookkeeping on the compressed state, next-stage input (both tiles, FP32),
-// particle-2 diagonal D (FP64).
-template <int NN>
+// RK4 bookkeeping on the compressed state, next-stage input (both tiles, in
+// the storage type TT), particle-2 diagonal D (FP64).
+template <int NN, typename TT = float>
 __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
 {
+    using T2 = typename Cx2<TT>::T;
     if (!*s.d.active) return;
     const Dev &d = s.d;
     if (blockIdx.x >= s.npairs) {
@@ -149,11 +175,11 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
     const bool diag = rc.x == rc.y;
     extern __shared__ double2 smd[];
     double2 *Gs = smd;                                 // n x GLD
-    float2 *Wrc = reinterpret_cast<float2 *>(Gs + n * GLD);  // [c_l][r_l] = W[R0+r_l][C0+c_l]
-    float2 *Wcr = Wrc + kTB * (kTB + 1);               // [r_l][c_l] = W[C0+c_l][R0+r_l]
+    T2 *Wrc = reinterpret_cast<T2 *>(Gs + n * GLD);    // [c_l][r_l] = W[R0+r_l][C0+c_l]
+    T2 *Wcr = Wrc + kTB * (kTB + 1);                   // [r_l][c_l] = W[C0+c_l][R0+r_l]
     double2 *Ks = reinterpret_cast<double2 *>(Wcr + kTB * (kTB + 1));  // [c_l][r_l] tmp_next (or K), rows of KLD
     __shared__ int site[NN];
-    const float *Wg = s.W + t * 2 * s.n4;
+    const TT *Wg = reinterpret_cast<const TT *>(s.W) + t * 2 * s.n4;
     const double2 *G1 = (k & 1) ? d.G1t1 : d.G1t0;
     if (threadIdx.x < NN) site[threadIdx.x] = threadIdx.x % Ns;
 #pragma unroll 4
@@ -166,10 +192,10 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
         const int rl = e % kTB, cl = e / kTB;
         // W[R0+rl][C0+cl] at (c*2+part)*n2 + r: contiguous in rl
         const long long b1 = (long long)(C0 + cl) * 2 * n2 + R0 + rl;
-        Wrc[cl * (kTB + 1) + rl] = make_float2(Wg[b1], Wg[b1 + n2]);
+        Wrc[cl * (kTB + 1) + rl] = mk2<TT>(Wg[b1], Wg[b1 + n2]);
         // W[C0+rl'][R0+cl'] with rl' = rl as the row offset inside block C
         const long long b2 = (long long)(R0 + cl) * 2 * n2 + C0 + rl;
-        Wcr[cl * (kTB + 1) + rl] = make_float2(Wg[b2], Wg[b2 + n2]);
+        Wcr[cl * (kTB + 1) + rl] = mk2<TT>(Wg[b2], Wg[b2 + n2]);
     }
     __syncthreads();
 
@@ -230,8 +256,8 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
             const int cl = (threadIdx.x >> 5) + 8 * j;
             const int e = cl * kTB + rl;  // = threadIdx.x + 256 j
             const int nu1 = c0 + cl;
-            const float2 w1 = Wrc[cl * (kTB + 1) + rl];
-            const float2 w2 = Wcr[rl * (kTB + 1) + cl];
+            const T2 w1 = Wrc[cl * (kTB + 1) + rl];
+            const T2 w2 = Wcr[rl * (kTB + 1) + cl];
             const double2 C = make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
             const double2 g11 = Gs[mu1 * GLD + nu1];
             const double2 g1122 = c_mul(g11, g22);
@@ -274,9 +300,9 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
         const int rl = e % kTB, cl = e / kTB;
         const int r = R0 + rl, c = C0 + cl;
         const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
-        const float2 w1 = Wrc[cl * (kTB + 1) + rl];
+        const T2 w1 = Wrc[cl * (kTB + 1) + rl];
         // W[c][r] = Wcr at (row offset cl in block C -> index rl' = cl, col r -> cl' = rl)
-        const float2 w2 = Wcr[rl * (kTB + 1) + cl];
+        const T2 w2 = Wcr[rl * (kTB + 1) + cl];
         const double2 C = make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
         const int si = site[mu1], sj = site[mu2], sk = site[nu1], sl = site[nu2];
         const double2 g11 = Gs[mu1 * GLD + nu1], g22 = Gs[mu2 * GLD + nu2];
@@ -352,15 +378,15 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
         }
     }
     __syncthreads();
-    float *Out = sym_out(s, k) + t * 2 * s.n4;
+    TT *Out = sym_out<TT>(s, k) + t * 2 * s.n4;
     // tile (R, C): fastest index mu1 = r % n follows rl
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
         const int r = R0 + rl, c = C0 + cl;
         const double2 v = Ks[cl * KLD + rl];
         const long long o = tmp_index(n, r % n, r / n, c, 0);
-        Out[o] = float(v.x);
-        Out[o + n] = float(v.y);
+        Out[o] = TT(v.x);
+        Out[o + n] = TT(v.y);
     }
     if (!diag) {
         // tile (C, R): element (c, r) = conj(v); fastest index nu1 = c % n follows cl
@@ -369,14 +395,15 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
             const int r = R0 + rl, c = C0 + cl;
             const double2 v = Ks[cl * KLD + rl];
             const long long o = tmp_index(n, c % n, c / n, r, 0);
-            Out[o] = float(v.x);
-            Out[o + n] = float(-v.y);
+            Out[o] = TT(v.x);
+            Out[o + n] = TT(-v.y);
         }
     }
 }
 
 // Full FP64 state (device orbital layout, Y2 of the general engine) -> Yc,
-// TMPb (stage-0 input) and D.  One block per tile pair and tensor.
+// TMPb (stage-0 input, storage type TT) and D.  One block per tile pair and tensor.
+template <typename TT>
 __global__ void k_sym_pack(SymDev s, const double2 *Yfull)
 {
     const int n = s.n;
@@ -386,7 +413,7 @@ __global__ void k_sym_pack(SymDev s, const double2 *Yfull)
     const int R0 = rc.x * kTB, C0 = rc.y * kTB;
     const double2 *Y = Yfull + t * s.n4;
     double2 *Yc = s.Yc + ((long long)t * s.npairs + p) * kTB * kTB;
-    float *Out = s.TMPb + t * 2 * s.n4;
+    TT *Out = reinterpret_cast<TT *>(s.TMPb) + t * 2 * s.n4;
     double2 *Dt = s.d.D + t * n3;
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
@@ -396,13 +423,13 @@ __global__ void k_sym_pack(SymDev s, const double2 *Yfull)
         const double2 v = Y[(long long)c + n2 * mu1 + n3 * mu2];
         Yc[e] = v;
         long long o = tmp_index(n, mu1, mu2, c, 0);
-        Out[o] = float(v.x);
-        Out[o + n] = float(v.y);
+        Out[o] = TT(v.x);
+        Out[o + n] = TT(v.y);
         if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = v;
         if (rc.x != rc.y) {
             o = tmp_index(n, nu1, nu2, r, 0);
-            Out[o] = float(v.x);
-            Out[o + n] = float(-v.y);
+            Out[o] = TT(v.x);
+            Out[o + n] = TT(-v.y);
             if (nu2 == mu2) Dt[((long long)nu1 * n + mu1) * n + nu2] = c_conj(v);
         }
     }

@@ -45,14 +45,18 @@ enum g12_precision {
     G12_PREC_BF16OZ = 2,  /* tcgen05 kind::f16: exact 8-bit integer digits in bf16 (4 per operand,
                              10 products, exact FP32 partial sums), unbiased; the accurate mixed mode */
     G12_PREC_FP32 = 3,    /* symmetric engine with an FP32 CUDA-core contraction (checker) */
-    G12_PREC_TF32X6 = 4   /* tcgen05 kind::tf32: 3 tf32 pieces per operand, 6 products */
+    G12_PREC_TF32X6 = 4,  /* tcgen05 kind::tf32: 3 tf32 pieces per operand, 6 products */
+    G12_PREC_FP64SYM = 5  /* symmetric engine entirely in FP64 (FP64 CUDA-core contraction,
+                             FP64 stage input and intermediate): the symmetric formulation
+                             without any reduced precision */
 };
-/* The mixed modes (BF16OZ, TF32X3, TF32X6, FP32) use the symmetric engine: they
+/* The mixed modes (BF16OZ, TF32X3, TF32X6, FP32) and FP64SYM use the symmetric engine: they
  * require the physical G2 symmetries G2[mu2 mu1; nu2 nu1] = G2[mu1 mu2; nu1 nu2]
  * and G2[nu1 nu2; mu1 mu2] = conj(G2[mu1 mu2; nu1 nu2]) (every state reached
  * from G2 = 0 has them; set_state keeps the upper 32 x 32 blocks of G2 seen as
  * an n^2 x n^2 matrix) and keep the RK4 state in FP64.  n = Ns*Nb must be 16 or
- * 32 for the tensor-core modes and 8, 16, 32 or 64 for FP32.  TF32X3/TF32X6
+ * 32 for the tensor-core modes, 8, 16, 32 or 64 for FP32 and 8, 16 or 32 for
+ * FP64SYM.  TF32X3/TF32X6
  * inherit the tensor cores' biased FP32 accumulation (about -4e-8 relative per
  * contraction on B200), which accumulates into a linear phase drift of G1;
  * BF16OZ keeps every partial sum an exact integer and has no such bias. */

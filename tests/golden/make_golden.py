@@ -7,7 +7,8 @@ oracle/_ref/g12_ref for full Main.cpp runs).  Inputs are seeded random
 complex arrays or the physics configurations listed below.
 
 Run from the repository root:  python tests/golden/make_golden.py
-(``python tests/golden/make_golden.py energy`` writes energy_pin.npz alone).
+(``python tests/golden/make_golden.py energy`` writes energy_pin.npz alone;
+``... baseline [name ...]`` the full-length benchmark-configuration runs).
 """
 import os
 import sys
@@ -101,6 +102,56 @@ def full_runs():
         print(name, "T =", traj.shape[0], "max|G2| =", float(np.max(np.abs(r["g2xx"]))))
 
 
+# The benchmark configurations at their stated lengths (the reference's own
+# RK_solver.h:96 loop, AS.h:63 switching first).  Config 2 leaves the switching
+# parameters at the reference defaults (AS_rate 3, AS_midpoint 25: 1373
+# switching steps); config 3 (n = 32) uses a shortened switching phase
+# (AS_rate 0.5, AS_midpoint 3: 234 steps) so that the compiled reference
+# finishes it in minutes, then 20 RK4 steps.  The pulse of config 2 and the
+# quench of config 3 stay masked by the reference's t < 50 gate.
+BASELINE_RUNS = {
+    "run_c1_full": Config(Ns=4, Nb=1, Nq=2, time_steps=2000, U=1.0, t1=1.0, t2=0.0, dt=0.02,
+                          AS_rate=0.5, AS_midpoint=10, q_type="full", quench_strength=1.0),
+    "run_c2_full": Config(Ns=8, Nb=2, Nq=3, time_steps=5000, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True,
+                          vlaw="inv", q_type="pulse", quench_strength=2.0, quench_rate=2,
+                          quench_on_midpoint=15, quench_off_midpoint=25),
+    "run_c3_20": Config(Ns=16, Nb=2, Nq=4, time_steps=20, U=1.5, t1=1.0, t2=0.3, dt=0.01, EHM=True,
+                        vlaw="inv", q_type="full", quench_strength=1.5, AS_rate=0.5, AS_midpoint=3),
+}
+# seeded complex test vectors for the G2 checksums (projections) of large runs
+N_PROJ = 8
+
+
+def g2_projections(G2, seed=7):
+    """N_PROJ linear functionals of a G2 tensor (reference layout): a checksum
+    of the full state that stays small for n = 16 and 32."""
+    rng = np.random.default_rng(seed)
+    P = rng.standard_normal((N_PROJ, G2.size)) + 1j * rng.standard_normal((N_PROJ, G2.size))
+    return P @ G2.reshape(-1)
+
+
+def baseline_runs(names=None):
+    for name, cfg in BASELINE_RUNS.items():
+        if names and name not in names:
+            continue
+        with tempfile.TemporaryDirectory() as d:
+            r = run_reference_exe(cfg, d, timeout=4 * 3600)
+        traj = r["traj"]
+        T = traj.shape[0]
+        every = 1 if T <= 40 else 25
+        keep = {"g0": r["g0"], "g1_as": r["g1_as"], "dipole": r["dipole"], "T": np.array(T),
+                "every": np.array(every), "traj_sub": traj[::every], "traj_last": traj[-1],
+                "g2xx_as_proj": g2_projections(r["g2xx_as"]), "g2xy_as_proj": g2_projections(r["g2xy_as"]),
+                "g2xx_proj": g2_projections(r["g2xx"]), "g2xy_proj": g2_projections(r["g2xy"]),
+                "g2_norms": np.array([np.linalg.norm(r[k]) for k in ("g2xx_as", "g2xy_as", "g2xx", "g2xy")])}
+        if cfg.n <= 16:
+            keep["g2xx"], keep["g2xy"] = r["g2xx"], r["g2xy"]
+        for k, v in cfg.__dict__.items():
+            keep["cfg_" + k] = np.array(v)
+        np.savez_compressed(os.path.join(OUT, f"{name}.npz"), **keep)
+        print(name, "T =", T, "max|G2| =", float(np.max(np.abs(r["g2xx"]))), flush=True)
+
+
 # total-energy pin: the state after adiabatic switching and the state after the
 # T RK4 iterations of a run (constant U, quench masked by the t < 50 gate), at
 # two step sizes over the same simulated time
@@ -151,7 +202,11 @@ if __name__ == "__main__":
     if sys.argv[1:] == ["energy"]:
         energy_pin()
         sys.exit(0)
+    if sys.argv[1:2] == ["baseline"]:
+        baseline_runs(sys.argv[2:])
+        sys.exit(0)
     per_routine(Reference())
     full_runs()
+    baseline_runs()
     energy_pin()
     sample_input()

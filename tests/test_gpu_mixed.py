@@ -114,3 +114,30 @@ def test_particle_number_conserved(g12, prec, tol):
     assert rc == 0
     N = g12.particle_number(traj)
     assert np.max(np.abs(N - N[0])) <= tol * abs(N[0]), np.max(np.abs(N - N[0]))
+
+
+@pytest.mark.parametrize("Ns,Nb", [(8, 2), (16, 2), (4, 2)])
+def test_fp64sym_rhs_vs_oracle(g12, oracle, Ns, Nb):
+    """The symmetric engine in FP64 (one contraction per tensor, compressed
+    state) reproduces the reference's RHS terms to FP64 round-off."""
+    cfg = Config(Ns=Ns, Nb=Nb, Nq=2, U=1.4, t2=0.3, EHM=True, vlaw="inv")
+    rng = np.random.default_rng(Ns * Nb + 11)
+    G1, XX, XY = physical_state(rng, Ns, Nb)
+    with g12.Context(params_of(g12, cfg), "fp64sym") as ctx:
+        got = ctx.rhs(G1, XX, XY, 1.3, 0.5, 2)
+    ref = oracle_rhs(oracle, cfg, G1, XX, XY, 1.3, 0.5, 2)
+    for k in ("h", "comm1", "Ix", "K1", "K2xx", "K2xy"):
+        assert rel_err(got[k], ref[k]) <= 1e-12, (k, rel_err(got[k], ref[k]))
+
+
+def test_fp64sym_propagation_vs_fp64(g12):
+    cfg = Config(Ns=8, Nb=2, Nq=3, time_steps=300, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, vlaw="inv",
+                 q_type="pulse", quench_strength=2.0, quench_rate=2, quench_on_midpoint=15,
+                 quench_off_midpoint=25, AS_rate=0.3, AS_midpoint=2.0)
+    p = params_of(g12, cfg)
+    G0 = g12.make_G0(p)
+    ref, rc0, st0 = _run(g12, p, "fp64", G0, 300)
+    got, rc1, st1 = _run(g12, p, "fp64sym", G0, 300)
+    assert rc0 == 0 and rc1 == 0
+    assert rel_err(got, ref) <= 1e-11
+    assert rel_err(st1[1], st0[1]) <= 1e-10 and rel_err(st1[2], st0[2]) <= 1e-10

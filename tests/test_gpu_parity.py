@@ -116,6 +116,48 @@ def test_full_run_vs_reference_golden(g12, name):
     assert dipole_err(g12.dipole(traj), g["dipole"], traj) <= RUN_TOL
 
 
+def _g2_projections(G2):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(ROOT, "tests", "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg.g2_projections(G2)
+
+
+@pytest.mark.parametrize("name", ["run_c1_full", "run_c2_full", "run_c3_20"])
+def test_benchmark_config_vs_reference_golden(g12, name):
+    """The benchmark configurations at their stated lengths against the
+    compiled reference (RK_solver.h:96-216 after AS.h:63-214): config 1
+    (n = 4, 2000 steps), config 2 (n = 16, EHM U/(1+r), 5001 iterations) and
+    config 3 (n = 32, 20 steps after a shortened switching phase).  G1 every
+    25th snapshot and the last, the dipole, and the G2 state after switching
+    and at the end (in full for n <= 16, by seeded projections for n = 32)."""
+    g = load_golden(name + ".npz")
+    cfg = _cfg_from(g)
+    p = params_of(g12, cfg)
+    T = int(g["T"])
+    every = int(g["every"])
+    with g12.Context(p) as ctx:
+        ctx.set_state(g["g0"])
+        ctx.adiabatic_switch()
+        G1as, XXas, XYas = ctx.get_state()
+        traj, rc = ctx.propagate(g12.rk_iterations(p))
+        G1, XX, XY = ctx.get_state()
+    assert rc == 0 and traj.shape[0] == T
+    assert rel_err(G1as, g["g1_as"]) <= RUN_TOL
+    assert rel_err(traj[::every], g["traj_sub"]) <= RUN_TOL
+    assert rel_err(traj[-1], g["traj_last"]) <= RUN_TOL
+    assert dipole_err(g12.dipole(traj), g["dipole"], traj) <= RUN_TOL
+    norms = g["g2_norms"]
+    for i, (X, key) in enumerate(((XXas, "g2xx_as_proj"), (XYas, "g2xy_as_proj"), (XX, "g2xx_proj"),
+                                  (XY, "g2xy_proj"))):
+        assert abs(np.linalg.norm(X) - norms[i]) <= RUN_TOL * norms[i]
+        pr = _g2_projections(X)
+        assert np.max(np.abs(pr - g[key])) <= RUN_TOL * norms[i] * np.sqrt(X.size), key
+    if "g2xx" in g.files:
+        assert rel_err(XX, g["g2xx"]) <= RUN_TOL and rel_err(XY, g["g2xy"]) <= RUN_TOL
+
+
 def test_device_dipole_and_chunked_clock(g12):
     g = load_golden("run_quench_on.npz")
     cfg = _cfg_from(g)
