@@ -400,6 +400,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--no-extended", action="store_true")
     ap.add_argument("--no-full-run", action="store_true")
+    ap.add_argument("--no-writer", action="store_true")
     ap.add_argument("--skip-as", action="store_true",
                     help="start the timed steps from G0 (profiling runs); the cost of a step does not depend on the state")
     args = ap.parse_args()
@@ -459,22 +460,56 @@ def main():
     g1_err = float(np.max(np.abs(traj_mx - traj_fp)) / np.max(np.abs(traj_fp)))
     launches = mx.launches_per_step * K
 
-    # e2e through the C ABI with host buffers: the plain user call (no eviction aid)
+    # e2e through the C ABI with host buffers: the plain user call (no eviction
+    # aid), every host buffer in pinned memory
     import ctypes
-    traj_host = np.zeros((K, n, n), np.complex128)
+
+    import torch
+
+    def pinned(shape):
+        return torch.empty(shape, dtype=torch.complex128, pin_memory=True).numpy()
+
+    dp = ctypes.POINTER(ctypes.c_double)
+    ptr = lambda a: a.ctypes.data_as(dp)
+    S_in = [pinned(a.shape) for a in S]
+    for a, b in zip(S_in, S):
+        a[...] = b
+    S_out = [pinned(a.shape) for a in S]
+    traj_host = pinned((K, n, n))
     done = ctypes.c_int64()
+    L = g12.lib()
     barrier(pg)
     t0 = time.perf_counter()
-    mx.set_state(*S)
-    g12.lib().g12_propagate(mx.h, K, traj_host.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(done))
-    mx.get_state()
+    L.g12_set_state(mx.h, ptr(S_in[0]), ptr(S_in[1]), ptr(S_in[2]))
+    L.g12_propagate(mx.h, K, ptr(traj_host), ctypes.byref(done))
+    L.g12_get_state(mx.h, ptr(S_out[0]), ptr(S_out[1]), ptr(S_out[2]))
     t1 = time.perf_counter()
     e2e_s = allmax(pg, t1 - t0)
+    assert done.value == K
     state_bytes = (n * n + 2 * n ** 4) * 16
     e2e = {"value": world * K / e2e_s, "unit": "steps/s", "h2d_bytes_per_step": state_bytes / K,
            "d2h_bytes_per_step": n * n * 16 + state_bytes / K,
-           "note": "set_state + propagate(K, per-step G1 snapshots to host) + get_state, wall clock, "
-                   "as a user calls it (no L2 eviction between steps)"}
+           "note": f"g12_set_state + g12_propagate({K} steps, per-step G1 snapshots to host) + g12_get_state, "
+                   "pinned host buffers, wall clock, as a user calls it (no L2 eviction between steps); the "
+                   "state upload and download (33.5 MB each) are spread over the K steps"}
+    # the reference's text output of a 10,000-step trajectory (write_to_file.h:52-69):
+    # real_/imag_G1.txt, n^2 rows x T columns, 6 significant digits
+    writer = None
+    if rank == 0 and not args.no_writer:
+        Tw = 10000
+        big = np.tile(traj_host[: min(K, Tw)], (Tw // min(K, Tw) + 1, 1, 1))[:Tw]
+        cwd = os.getcwd()
+        with tempfile.TemporaryDirectory() as d:
+            os.chdir(d)  # the reference writes real_/imag_<name> into the working directory
+            try:
+                t0 = time.perf_counter()
+                rc_w = L.g12_write_cfile2D(b"G1.txt", ptr(big), Tw, n * n)
+                tw = time.perf_counter() - t0
+            finally:
+                os.chdir(cwd)
+            size = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+        writer = {"snapshots": Tw, "n": n, "seconds": tw, "bytes": size, "status": rc_w,
+                  "threads": os.cpu_count(), "mb_per_s": size / tw / 1e6}
 
     # per-kernel device times (CUDA events around each launch on the library stream)
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
@@ -575,7 +610,7 @@ def main():
                        "mixed_rel_drift": float(abs(E_mx[0] - E_start[0]) / abs(E_start[0])),
                        "correlation_change": float(E_mx[3] - E_start[3]),
                        "note": "g12_total_energy before and after the timed steps (constant U, quench masked)"},
-            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline,
+            "e2e": e2e, "text_writer_n32_10k": writer, "gpu_launches": launches, "roofline": roofline, "step_roofline": step_roofline,
             "kernels": kernels, "cpu_baseline": cpu, "clocks": clk.summary(),
             "sections_printed_above": sections,
         }

@@ -141,3 +141,50 @@ def test_fp64sym_propagation_vs_fp64(g12):
     assert rc0 == 0 and rc1 == 0
     assert rel_err(got, ref) <= 1e-11
     assert rel_err(st1[1], st0[1]) <= 1e-10 and rel_err(st1[2], st0[2]) <= 1e-10
+
+
+# The benchmark configurations at their stated lengths, mixed engine against
+# the FP64 path from the same G0 (each through its own adiabatic switching):
+# the metric's bound, G1 error <= 1e-6 relative to max |G1| (and the dipole
+# likewise), over the whole trajectory.
+FULL_TOL = 1e-6
+
+
+def _full(g12, p, prec, T):
+    with g12.Context(p, prec) as ctx:
+        ctx.set_state(g12.make_G0(p))
+        ctx.adiabatic_switch()
+        traj, rc = ctx.propagate(T)
+    return traj, rc
+
+
+@pytest.mark.parametrize("gate", [0.0, 50.0])
+def test_bf16oz_config2_full_length(g12, gate):
+    """Ns=8, Nb=2 (n=16), t2=0.5, U=2, EHM U/(1+r), pulse 2.0 on Nq=3 (rate 2,
+    on/off 15/25), dt=0.01, 5000 steps = 5001 iterations.  gate 0: the pulse
+    acts (quench_gate extension); gate 50: the reference's own t < 50 gate."""
+    p = g12.make_params(Ns=8, Nb=2, Nq=3, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, v_law="inv",
+                        q_type="pulse", quench_strength=2.0, quench_rate=2.0, quench_on_midpoint=15.0,
+                        quench_off_midpoint=25.0, time_steps=5000, quench_gate=gate)
+    T = g12.rk_iterations(p)
+    assert T == 5001
+    ref, rc0 = _full(g12, p, "fp64", T)
+    got, rc1 = _full(g12, p, "bf16oz", T)
+    assert rc0 == 0 and rc1 == 0
+    assert rel_err(got, ref) <= FULL_TOL, rel_err(got, ref)
+    pr, pg = g12.dipole(ref), g12.dipole(got)
+    assert np.max(np.abs(pg - pr)) <= FULL_TOL * max(np.max(np.abs(pr)), np.max(np.abs(ref)))
+
+
+def test_bf16oz_config3_full_length(g12):
+    """Ns=16, Nb=2 (n=32), t2=0.3, U=1.5, EHM U/(1+r), full quench 1.5 on Nq=4
+    (switched on at t >= 50), dt=0.01, 10,000 steps."""
+    p = g12.make_params(Ns=16, Nb=2, Nq=4, time_steps=10000, U=1.5, t1=1.0, t2=0.3, dt=0.01, EHM=True,
+                        v_law="inv", q_type="full", quench_strength=1.5)
+    T = g12.rk_iterations(p)
+    ref, rc0 = _full(g12, p, "fp64", T)
+    got, rc1 = _full(g12, p, "bf16oz", T)
+    assert rc0 == 0 and rc1 == 0
+    assert rel_err(got, ref) <= FULL_TOL, rel_err(got, ref)
+    pr, pg = g12.dipole(ref), g12.dipole(got)
+    assert np.max(np.abs(pg - pr)) <= FULL_TOL * max(np.max(np.abs(pr)), 1e-12), np.max(np.abs(pg - pr))
