@@ -23,6 +23,10 @@ thread_local std::string g_create_error;
 
 struct LaunchCfg {
     ApplyCfg ab, cd;
+    bool tc = false;         // FP64 tensor-core (DMMA) two-body halves
+    ApplyTcCfg tcc{};
+    size_t tc_ab_smem = 0, tc_cd_smem = 0;
+    dim3 tc_grid;
     int ab_threads, cd_threads;
     size_t ab_smem, cd_smem, prep_smem, g1_smem;
     dim3 apply_grid;
@@ -207,6 +211,19 @@ int ensure_sched(g12_ctx *ctx, long long steps)
     return G12_OK;
 }
 
+// The two halves of the FP64 two-body commutator with the fused epilogue:
+// q = 0 rows (particle indices), q = 1 columns + epilogue; -1 both.
+void enqueue_apply(const LaunchCfg &lc, const Dev &d, int k, cudaStream_t s, int q = -1)
+{
+    if (lc.tc) {
+        if (q != 1) k_apply_tc<false><<<lc.tc_grid, lc.tcc.threads, lc.tc_ab_smem, s>>>(d, k, lc.tcc);
+        if (q != 0) k_apply_tc<true><<<lc.tc_grid, lc.tcc.threads, lc.tc_cd_smem, s>>>(d, k, lc.tcc);
+    } else {
+        if (q != 1) k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, s>>>(d, k, lc.ab);
+        if (q != 0) k_apply<true><<<lc.apply_grid, lc.cd_threads, lc.cd_smem, s>>>(d, k, lc.cd);
+    }
+}
+
 // One RK4 step.  k_g1 of stage k only feeds k_prep of stage k+1, so it runs
 // on a side branch (s2) concurrently with the two-body kernels of stage k.
 void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
@@ -240,8 +257,7 @@ void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
         cudaEventRecord(ctx->ev_join, ctx->s2);
         if (d.gate) {
             if (ctx->prec == G12_PREC_FP64) {
-                k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, s>>>(d, k, lc.ab);
-                k_apply<true><<<lc.apply_grid, lc.cd_threads, lc.cd_smem, s>>>(d, k, lc.cd);
+                enqueue_apply(lc, d, k, s);
             } else {
                 mixed_enqueue_stage(ctx->mixed, d, k, ctx->prec, s);
             }
@@ -454,6 +470,14 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     lc.g1_blocks = g1_blocks(n2);
     lc.g1_smem = g1_smem(n2);
     lc.steps_per_graph = n <= 8 ? 8 : (n <= 32 ? 4 : 1);
+    lc.tc = apply_tc_ok(n);
+    if (lc.tc) {
+        lc.tcc = make_apply_tc_cfg(n, &lc.tc_ab_smem, &lc.tc_cd_smem);
+        lc.tc_grid = dim3(unsigned((n2 + lc.tcc.NB - 1) / lc.tcc.NB), 2, 1);
+        if (!ck(ctx, cudaFuncSetAttribute(k_apply_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.tc_ab_smem)), "attr") ||
+            !ck(ctx, cudaFuncSetAttribute(k_apply_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.tc_cd_smem)), "attr"))
+            return fail(G12_ERR_CUDA);
+    }
     if (!ck(ctx, cudaFuncSetAttribute(k_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.ab_smem)), "attr") ||
         !ck(ctx, cudaFuncSetAttribute(k_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.cd_smem)), "attr") ||
         !ck(ctx, cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.prep_smem)), "attr") ||
@@ -644,8 +668,7 @@ extern "C" int g12_rhs(g12_ctx *ctx, const double *G1, const double *G2xx, const
     k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s>>>(dd, 0);
     if (dd.gate) {
         if (ctx->prec == G12_PREC_FP64) {
-            k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, ctx->s>>>(dd, 0, lc.ab);
-            k_apply<true><<<lc.apply_grid, lc.cd_threads, lc.cd_smem, ctx->s>>>(dd, 0, lc.cd);
+            enqueue_apply(lc, dd, 0, ctx->s);
         } else {
             mixed_enqueue_stage(ctx->mixed, dd, 0, ctx->prec, ctx->s);
         }
@@ -718,6 +741,7 @@ extern "C" int32_t g12_set_l2_eviction(g12_ctx *ctx, int64_t bytes)
 namespace {
 
 const char *kFp64Names[] = {"k_step_begin", "k_prep", "k_g1", "k_apply<rows>", "k_apply<cols+epilogue>"};
+const char *kFp64TcNames[] = {"k_step_begin", "k_prep", "k_g1", "k_apply_tc<rows>", "k_apply_tc<cols+epilogue>"};
 
 }  // namespace
 
@@ -726,7 +750,7 @@ extern "C" const char *g12_kernel_name(const g12_ctx *ctx, int32_t kind)
     if (!ctx) return "";
     if (ctx->prec != G12_PREC_FP64 && kind >= 3) return mixed_kernel_name(ctx->mixed, kind - 3);
     if (kind < 0 || kind >= 5) return "";
-    return kFp64Names[kind];
+    return ctx->lc.tc ? kFp64TcNames[kind] : kFp64Names[kind];
 }
 
 extern "C" int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms, int32_t *calls_per_step, int32_t cap)
@@ -771,8 +795,8 @@ extern "C" int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms
             if (!fused) timed(2, [&] { k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s>>>(d, k); });
             if (!d.gate) continue;
             if (ctx->prec == G12_PREC_FP64) {
-                timed(3, [&] { k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, ctx->s>>>(d, k, lc.ab); });
-                timed(4, [&] { k_apply<true><<<lc.apply_grid, lc.cd_threads, lc.cd_smem, ctx->s>>>(d, k, lc.cd); });
+                timed(3, [&] { enqueue_apply(lc, d, k, ctx->s, 0); });
+                timed(4, [&] { enqueue_apply(lc, d, k, ctx->s, 1); });
             } else {
                 for (int q = 0; q < mixed_kernel_kinds(ctx->mixed); ++q)
                     timed(3 + q, [&] { mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, q, ctx->s, fused); });

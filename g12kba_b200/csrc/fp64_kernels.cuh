@@ -35,6 +35,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "internal.h"
 
 namespace g12 {
@@ -451,6 +453,79 @@ struct ApplyCfg {
     int NP, LD, S, NB;
 };
 
+// Fused epilogue of one element G2[r; nu1 nu2] (r = mu1 + n mu2) of the
+// column half: C = TAB - Y (Y = (M H2) at that element), Psi, Pi, K2
+// (G1_G2_t_step.h:55-86) and the RK4 bookkeeping (RK_solver.h:137-139,
+// 209-213).  Gs: the stage's G1, n x n row-major (shared memory).
+struct ApplyEpi {
+    long long r;
+    StageP st;
+    int mu1, mu2, si, sj;
+    double U, wij;
+    __device__ __forceinline__ ApplyEpi(const Dev &d, const StageP &st_, long long r_) : r(r_), st(st_)
+    {
+        const int n = d.n, Ns = d.Ns;
+        U = st.U;
+        mu1 = int(r % n);
+        mu2 = int(r / n);
+        si = mu1 % Ns;
+        sj = mu2 % Ns;
+        wij = U * double(si == sj) + vdist(d, si, sj);
+    }
+    __device__ __forceinline__ double vdist(const Dev &d, int s1, int s2) const
+    {
+        const int m = abs(s1 - s2);
+        return (m >= 1 && m <= d.nv) ? U * d.law[m - 1] : 0.0;
+    }
+    __device__ __forceinline__ void element(const Dev &d, int k, int t, int nu1, int nu2, double2 y,
+                                            const double2 *Gs) const
+    {
+        const int n = d.n, Ns = d.Ns;
+        const long long n2 = d.n2, n4 = d.n4;
+        const int sk = nu1 % Ns, sl = nu2 % Ns;
+        const double2 *Rt1 = d.Rt + ((long long)mu1 * n) * Ns;  // + nu1*Ns + s
+        const double2 *Rt2 = d.Rt + ((long long)mu2 * n) * Ns;  // + nu2*Ns + s
+        const double2 *Qt = d.Q + t * d.n3;
+        const long long x = r * n2 + nu1 + (long long)n * nu2;
+        const double2 C = c_sub(d.TAB[t * n4 + x], y);
+        const double2 g11 = Gs[mu1 * n + nu1], g22 = Gs[mu2 * n + nu2];
+        const double wd = wij - (U * double(sk == sl) + vdist(d, sk, sl));
+        double2 psi = c_scale(c_mul(g11, g22), wd);
+        psi = c_add(psi, c_i(c_mul(g22, c_sub(Rt1[nu1 * Ns + sj], Rt1[nu1 * Ns + sl]))));
+        psi = c_add(psi, c_i(c_mul(g11, c_sub(Rt2[nu2 * Ns + si], Rt2[nu2 * Ns + sk]))));
+        if (t == 0) {
+            psi = c_sub(psi, c_scale(c_mul(g11, g22), U * (double(mu1 == mu2) - double(nu1 == nu2))));
+            const double2 e1 = c_sub(c_mul(Gs[mu1 * n + mu2], Gs[mu2 * n + nu1]),
+                                     c_mul(Gs[mu1 * n + nu2], Gs[nu2 * n + nu1]));
+            const double2 e2 = c_sub(c_mul(Gs[mu2 * n + mu1], Gs[mu1 * n + nu2]),
+                                     c_mul(Gs[mu2 * n + nu1], Gs[nu1 * n + nu2]));
+            psi = c_add(psi, c_scale(c_mi(c_add(c_mul(g22, e1), c_mul(g11, e2))), U));
+        }
+        const long long q1 = ((long long)mu1 * n + nu1) * n, q2 = ((long long)nu2 * n + mu2) * n;
+        const double2 pi = c_mul(g22, c_sub(Qt[q1 + mu2], Qt[q1 + nu2]));
+        const double2 piP = c_mul(Gs[nu1 * n + mu1], c_sub(Qt[q2 + nu1], Qt[q2 + mu1]));
+        const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
+        if (d.debug) {
+            d.TMP0[t * n4 + x] = K;
+            return;
+        }
+        double2 *RKt = d.RK2 + t * n4;
+        double2 *Yt = d.Y2 + t * n4;
+        double2 *Dt = d.D + t * d.n3;
+        const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : RKt[x], c_scale(K, st.w));
+        if (k < 3) {
+            RKt[x] = rk;
+            const double2 tn = c_add(Yt[x], c_scale(K, st.c_next));
+            g2_next(d, k)[t * n4 + x] = tn;
+            if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = tn;
+        } else {
+            const double2 yn = c_add(Yt[x], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
+            Yt[x] = yn;
+            if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = yn;
+        }
+    }
+};
+
 template <bool CD>
 __device__ __forceinline__ void apply_body(const Dev &d, int k, const ApplyCfg &cfg, int bx, int t)
 {
@@ -550,69 +625,16 @@ __device__ __forceinline__ void apply_body(const Dev &d, int k, const ApplyCfg &
     if (!live) return;
     // ---- fused epilogue (CD) ----
     const StageP st = d.cur->st[k];
-    const double U = st.U;
-    const int Ns = d.Ns;
-    const long long r = m0 + mat;
-    const int mu1 = int(r % n), mu2 = int(r / n);
-    const int si = mu1 % Ns, sj = mu2 % Ns;
-    const double2 *Tt = d.TAB + t * n4;
-    const double2 *Qt = d.Q + t * d.n3;
-    double2 *RKt = d.RK2 + t * n4;
-    double2 *Yt = d.Y2 + t * n4;
-    double2 *Dt = d.D + t * d.n3;
-    double2 *Nt = g2_next(d, k) + t * n4;
-    double2 *Kdbg = d.TMP0 + t * n4;
-    auto vdist = [&](int s1, int s2) -> double {
-        const int m = abs(s1 - s2);
-        return (m >= 1 && m <= d.nv) ? U * d.law[m - 1] : 0.0;
-    };
-    const double wij = U * double(si == sj) + vdist(si, sj);
-    const double2 *Rt1 = d.Rt + ((long long)mu1 * n) * Ns;  // + nu1*Ns + s
-    const double2 *Rt2 = d.Rt + ((long long)mu2 * n) * Ns;  // + nu2*Ns + s
+    const ApplyEpi ep(d, st, m0 + mat);
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int nu2 = ti + S * a;
         if (nu2 >= n) continue;
-        const int sl = nu2 % Ns;
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const int nu1 = tj + S * b;
             if (nu1 >= n) continue;
-            const int sk = nu1 % Ns;
-            const long long x = r * n2 + nu1 + (long long)n * nu2;
-            const double2 C = c_sub(Tt[x], acc[a][b]);
-            const double2 g11 = Gs[mu1 * n + nu1], g22 = Gs[mu2 * n + nu2];
-            const double wd = wij - (U * double(sk == sl) + vdist(sk, sl));
-            double2 psi = c_scale(c_mul(g11, g22), wd);
-            psi = c_add(psi, c_i(c_mul(g22, c_sub(Rt1[nu1 * Ns + sj], Rt1[nu1 * Ns + sl]))));
-            psi = c_add(psi, c_i(c_mul(g11, c_sub(Rt2[nu2 * Ns + si], Rt2[nu2 * Ns + sk]))));
-            if (t == 0) {
-                psi = c_sub(psi, c_scale(c_mul(g11, g22), U * (double(mu1 == mu2) - double(nu1 == nu2))));
-                const double2 e1 = c_sub(c_mul(Gs[mu1 * n + mu2], Gs[mu2 * n + nu1]),
-                                         c_mul(Gs[mu1 * n + nu2], Gs[nu2 * n + nu1]));
-                const double2 e2 = c_sub(c_mul(Gs[mu2 * n + mu1], Gs[mu1 * n + nu2]),
-                                         c_mul(Gs[mu2 * n + nu1], Gs[nu1 * n + nu2]));
-                psi = c_add(psi, c_scale(c_mi(c_add(c_mul(g22, e1), c_mul(g11, e2))), U));
-            }
-            const long long q1 = ((long long)mu1 * n + nu1) * n, q2 = ((long long)nu2 * n + mu2) * n;
-            const double2 pi = c_mul(g22, c_sub(Qt[q1 + mu2], Qt[q1 + nu2]));
-            const double2 piP = c_mul(Gs[nu1 * n + mu1], c_sub(Qt[q2 + nu1], Qt[q2 + mu1]));
-            const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
-            if (d.debug) {
-                Kdbg[x] = K;
-                continue;
-            }
-            const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : RKt[x], c_scale(K, st.w));
-            if (k < 3) {
-                RKt[x] = rk;
-                const double2 tn = c_add(Yt[x], c_scale(K, st.c_next));
-                Nt[x] = tn;
-                if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = tn;
-            } else {
-                const double2 yn = c_add(Yt[x], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
-                Yt[x] = yn;
-                if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = yn;
-            }
+            ep.element(d, k, t, nu1, nu2, acc[a][b], Gs);
         }
     }
 }
@@ -621,6 +643,186 @@ template <bool CD>
 static __global__ void __launch_bounds__(256) k_apply(Dev d, int k, ApplyCfg cfg)
 {
     apply_body<CD>(d, k, cfg, blockIdx.x, blockIdx.y);
+}
+
+// FP64 tensor-core version of the two halves (n = 16 .. 48): mma.sync
+// m8n8k4 f64 (DMMA).  Each warp computes a 16 x 16 complex block of
+// Y = L X + X R for one matrix (2 x 2 tiles of 8 x 8, real and imaginary parts,
+// 4 real products per complex product, accumulated in FP64 like the FMA
+// path).  Operands live in shared memory as separate real and imaginary
+// planes of NP x LDD doubles, NP = n rounded up to 16 (zero padding), LDD = 12
+// mod 16, so the fragment loads of the row-major A and column-major B operands
+// touch each 8-byte bank at most twice per warp.  Results return through the
+// X planes; the column half then runs the same per-element epilogue
+// (ApplyEpi) as the FMA path, with consecutive threads on consecutive nu1.
+struct ApplyTcCfg {
+    int NP, LDD, NB, threads;
+};
+
+inline bool apply_tc_ok(int n) { return n >= 16 && n <= 48; }
+
+inline ApplyTcCfg make_apply_tc_cfg(int n, size_t *smem_ab, size_t *smem_cd)
+{
+    ApplyTcCfg c;
+    c.NP = (n + 15) / 16 * 16;
+    c.LDD = c.NP + 12;
+    const int tpm = (c.NP / 16) * (c.NP / 16);
+    const size_t plane = size_t(c.NP) * c.LDD * sizeof(double);
+    c.NB = std::max(1, std::min(n * n, 16 / tpm));
+    while (c.NB > 1 && (4 + 2 * size_t(c.NB)) * plane + size_t(n) * n * sizeof(double2) > 200 * 1024) c.NB--;
+    c.threads = c.NB * tpm * 32;
+    *smem_ab = (4 + 2 * size_t(c.NB)) * plane;
+    *smem_cd = *smem_ab + size_t(n) * n * sizeof(double2);
+    return c;
+}
+
+__device__ __forceinline__ void dmma_f64(double &c0, double &c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <bool CD>
+__device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTcCfg &cfg, int bx, int t)
+{
+    if (!*d.active) return;
+    const int n = d.n, NP = cfg.NP, LDD = cfg.LDD, NB = cfg.NB;
+    const long long n2 = d.n2, n4 = d.n4;
+    const long long m0 = (long long)bx * NB;
+    const int nm = int(min((long long)NB, n2 - m0));
+    const int PL = NP * LDD;
+    extern __shared__ double smtc[];
+    double *Lr = smtc, *Li = Lr + PL, *Rr = Li + PL, *Ri = Rr + PL;
+    double *Xp = Ri + PL;  // NB x (real, imaginary) planes
+    double2 *Gs = reinterpret_cast<double2 *>(Xp + 2 * NB * PL);  // CD only: n*n
+    const double2 *X = g2_stage(d, k) + t * n4;
+
+    // (L, R) = (h, h^T) for the rows, (h^T, h) for the columns
+    for (int x = threadIdx.x; x < NP * NP; x += blockDim.x) {
+        const int r = x / NP, c = x % NP;
+        const double2 v = (r < n && c < n) ? d.h[r * n + c] : make_double2(0.0, 0.0);
+        const int lo = CD ? c * LDD + r : r * LDD + c, ro = CD ? r * LDD + c : c * LDD + r;
+        Lr[lo] = v.x;
+        Li[lo] = v.y;
+        Rr[ro] = v.x;
+        Ri[ro] = v.y;
+    }
+    if (NP != n)
+        for (int x = threadIdx.x; x < 2 * NB * PL; x += blockDim.x) Xp[x] = 0.0;
+    if (CD) {
+        const double2 *G1 = g1_stage(d, k);
+        for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[x] = G1[x];
+    }
+    __syncthreads();
+    if (!CD) {
+        // (mu2, mu1, cb) with cb fastest: NB contiguous entries per row of M
+        for (long long e = threadIdx.x; e < n2 * NB; e += blockDim.x) {
+            const int cb = int(e % NB);
+            const long long p = e / NB;  // mu1 + n*mu2
+            const int mu1 = int(p % n), mu2 = int(p / n);
+            if (cb < nm) {
+                const double2 v = X[p * n2 + m0 + cb];
+                double *P = Xp + 2 * cb * PL;
+                P[mu2 * LDD + mu1] = v.x;
+                P[PL + mu2 * LDD + mu1] = v.y;
+            }
+        }
+    } else {
+        for (long long e = threadIdx.x; e < (long long)nm * n2; e += blockDim.x) {
+            const int rb = int(e / n2), c = int(e % n2);
+            const int nu1 = c % n, nu2 = c / n;
+            const double2 v = X[(m0 + rb) * n2 + c];
+            double *P = Xp + 2 * rb * PL;
+            P[nu2 * LDD + nu1] = v.x;
+            P[PL + nu2 * LDD + nu1] = v.y;
+        }
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int TW = NP / 16, tpm = TW * TW;
+    const int mat = warp / tpm, wt = warp % tpm;
+    const int row0 = (wt / TW) * 16, col0 = (wt % TW) * 16;
+    const bool live = mat < nm;
+    double yr[2][2][2], yi[2][2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) yr[i][j][q] = yi[i][j][q] = 0.0;
+    if (live) {
+        const double *Xr = Xp + 2 * mat * PL, *Xi = Xr + PL;
+        auto step = [&](const double *Ar, const double *Ai, const double *Br, const double *Bi, int k0) {
+            double ar[2], ai[2], br[2], bi[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int o = (row0 + 8 * i + gid) * LDD + k0 + tig;
+                ar[i] = Ar[o];
+                ai[i] = Ai[o];
+            }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const int o = (k0 + tig) * LDD + col0 + 8 * j + gid;
+                br[j] = Br[o];
+                bi[j] = Bi[o];
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    dmma_f64(yr[i][j][0], yr[i][j][1], ar[i], br[j]);
+                    dmma_f64(yr[i][j][0], yr[i][j][1], -ai[i], bi[j]);
+                    dmma_f64(yi[i][j][0], yi[i][j][1], ar[i], bi[j]);
+                    dmma_f64(yi[i][j][0], yi[i][j][1], ai[i], br[j]);
+                }
+        };
+        for (int k0 = 0; k0 < NP; k0 += 4) step(Lr, Li, Xr, Xi, k0);  // L X
+        for (int k0 = 0; k0 < NP; k0 += 4) step(Xr, Xi, Rr, Ri, k0);  // X R
+    }
+    __syncthreads();  // every warp has read the X planes
+    if (live) {
+        double *Yr = Xp + 2 * mat * PL, *Yi = Yr + PL;
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int o = (row0 + 8 * i + gid) * LDD + col0 + 8 * j + 2 * tig + q;
+                    Yr[o] = yr[i][j][q];
+                    Yi[o] = yi[i][j][q];
+                }
+    }
+    __syncthreads();
+    if (!CD) {
+        double2 *T = d.TAB + t * n4;
+        for (long long e = threadIdx.x; e < n2 * NB; e += blockDim.x) {
+            const int cb = int(e % NB);
+            const long long p = e / NB;
+            const int mu1 = int(p % n), mu2 = int(p / n);
+            if (cb < nm) {
+                const double *P = Xp + 2 * cb * PL;
+                T[p * n2 + m0 + cb] = make_double2(P[mu2 * LDD + mu1], P[PL + mu2 * LDD + mu1]);
+            }
+        }
+        return;
+    }
+    const StageP st = d.cur->st[k];
+    for (long long e = threadIdx.x; e < (long long)nm * n2; e += blockDim.x) {
+        const int rb = int(e / n2), c = int(e % n2);
+        const int nu1 = c % n, nu2 = c / n;
+        const double *P = Xp + 2 * rb * PL;
+        const ApplyEpi ep(d, st, m0 + rb);
+        ep.element(d, k, t, nu1, nu2, make_double2(P[nu2 * LDD + nu1], P[PL + nu2 * LDD + nu1]), Gs);
+    }
+}
+
+template <bool CD>
+static __global__ void __launch_bounds__(512) k_apply_tc(Dev d, int k, ApplyTcCfg cfg)
+{
+    apply_tc_body<CD>(d, k, cfg, blockIdx.x, blockIdx.y);
 }
 
 // D[t][a][b][r] = Y2_t[a, r; b, r]

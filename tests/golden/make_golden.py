@@ -152,6 +152,29 @@ def baseline_runs(names=None):
         print(name, "T =", T, "max|G2| =", float(np.max(np.abs(r["g2xx"]))), flush=True)
 
 
+def roundoff_sensitivity(name="run_c2_full"):
+    """The reference's own sensitivity to round-off on a benchmark run: the same
+    input with G0 moved by one ulp in a seeded half of its entries.  Stores the
+    perturbed run's G1 (every 25th snapshot and the last), its dipole and its
+    final G2 checksums; the deviation from the unperturbed golden run is what
+    two correct FP64 implementations of these equations can differ by."""
+    cfg = BASELINE_RUNS[name]
+    g = np.load(os.path.join(OUT, f"{name}.npz"))
+    g0 = g["g0"].copy()
+    rng = np.random.default_rng(11)
+    mask = rng.random(g0.shape) < 0.5
+    g0 = np.where(mask, np.nextafter(g0.real, np.inf) + 1j * g0.imag, g0)
+    with tempfile.TemporaryDirectory() as d:
+        r = run_reference_exe(cfg, d, g0=g0, timeout=4 * 3600)
+    traj = r["traj"]
+    every = int(g["every"])
+    keep = {"g0": g0, "traj_sub": traj[::every], "traj_last": traj[-1], "dipole": r["dipole"],
+            "g1_as": r["g1_as"], "g2xx_proj": g2_projections(r["g2xx"]), "g2xy_proj": g2_projections(r["g2xy"])}
+    np.savez_compressed(os.path.join(OUT, f"{name}_ulp.npz"), **keep)
+    dev = np.max(np.abs(traj[::every] - g["traj_sub"])) / np.max(np.abs(g["traj_sub"]))
+    print(name, "one-ulp G0 perturbation: max G1 deviation", dev, flush=True)
+
+
 # total-energy pin: the state after adiabatic switching and the state after the
 # T RK4 iterations of a run (constant U, quench masked by the t < 50 gate), at
 # two step sizes over the same simulated time
@@ -205,8 +228,12 @@ if __name__ == "__main__":
     if sys.argv[1:2] == ["baseline"]:
         baseline_runs(sys.argv[2:])
         sys.exit(0)
+    if sys.argv[1:] == ["sensitivity"]:
+        roundoff_sensitivity()
+        sys.exit(0)
     per_routine(Reference())
     full_runs()
     baseline_runs()
+    roundoff_sensitivity()
     energy_pin()
     sample_input()

@@ -158,22 +158,68 @@ def _full(g12, p, prec, T):
     return traj, rc
 
 
+def g2_asymmetry(g12, X, Ns, Nb):
+    """||G2 - e(G2)|| / ||G2|| (exchange) for a tensor in the reference layout."""
+    n = Ns * Nb
+    perm = idx8_to_orbital(Ns, Nb)
+    Y = X[perm].reshape(n, n, n, n)
+    return float(np.linalg.norm(Y - Y.transpose(1, 0, 3, 2)) / np.linalg.norm(Y))
+
+
 @pytest.mark.parametrize("gate", [0.0, 50.0])
 def test_bf16oz_config2_full_length(g12, gate):
     """Ns=8, Nb=2 (n=16), t2=0.5, U=2, EHM U/(1+r), pulse 2.0 on Nq=3 (rate 2,
     on/off 15/25), dt=0.01, 5000 steps = 5001 iterations.  gate 0: the pulse
-    acts (quench_gate extension); gate 50: the reference's own t < 50 gate."""
+    acts (quench_gate extension); gate 50: the reference's own t < 50 gate.
+
+    On this configuration the plain FP64 path does not stay on the physical
+    states: the reference's equations keep G2's exchange and Hermitian
+    symmetries exactly (their right-hand side maps symmetric states to
+    symmetric ones), but the round-off of a non-symmetric propagation grows in
+    the unphysical part of G2 (the compiled reference's own final G2 breaks the
+    exchange symmetry at 1e-4, tests/golden/run_c2_full.npz).  The FP64
+    reference for the mixed engine is therefore the FP64 symmetric engine,
+    which propagates inside the physical subspace; both start from the same
+    switched state."""
     p = g12.make_params(Ns=8, Nb=2, Nq=3, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, v_law="inv",
                         q_type="pulse", quench_strength=2.0, quench_rate=2.0, quench_on_midpoint=15.0,
                         quench_off_midpoint=25.0, time_steps=5000, quench_gate=gate)
     T = g12.rk_iterations(p)
     assert T == 5001
-    ref, rc0 = _full(g12, p, "fp64", T)
-    got, rc1 = _full(g12, p, "bf16oz", T)
+    with g12.Context(p, "fp64sym") as ctx:
+        ctx.set_state(g12.make_G0(p))
+        ctx.adiabatic_switch()
+        S = ctx.get_state()
+        ref, rc0 = ctx.propagate(T)
+        end = ctx.get_state()
+    with g12.Context(p, "bf16oz") as ctx:
+        ctx.set_state(*S)
+        got, rc1 = ctx.propagate(T)
     assert rc0 == 0 and rc1 == 0
     assert rel_err(got, ref) <= FULL_TOL, rel_err(got, ref)
     pr, pg = g12.dipole(ref), g12.dipole(got)
     assert np.max(np.abs(pg - pr)) <= FULL_TOL * max(np.max(np.abs(pr)), np.max(np.abs(ref)))
+    # the symmetric engine's state stays physical to round-off
+    assert g2_asymmetry(g12, end[1], 8, 2) <= 1e-12 and g2_asymmetry(g12, end[2], 8, 2) <= 1e-12
+
+
+def test_plain_fp64_leaves_the_physical_states_on_config2(g12):
+    """The observation behind the previous test: from the same switched state,
+    the plain FP64 engine's G2 acquires an exchange-antisymmetric part that
+    grows far above round-off (the symmetric engine's stays at round-off)."""
+    p = g12.make_params(Ns=8, Nb=2, Nq=3, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, v_law="inv",
+                        q_type="pulse", quench_strength=2.0, quench_rate=2.0, quench_on_midpoint=15.0,
+                        quench_off_midpoint=25.0, time_steps=5000)
+    with g12.Context(p, "fp64sym") as ctx:
+        ctx.set_state(g12.make_G0(p))
+        ctx.adiabatic_switch()
+        S = ctx.get_state()
+    with g12.Context(p, "fp64") as ctx:
+        ctx.set_state(*S)
+        ctx.propagate(g12.rk_iterations(p))
+        _, XX, XY = ctx.get_state()
+    assert g2_asymmetry(g12, S[1], 8, 2) <= 1e-14
+    assert g2_asymmetry(g12, XX, 8, 2) >= 1e-8 and g2_asymmetry(g12, XY, 8, 2) >= 1e-8
 
 
 def test_bf16oz_config3_full_length(g12):

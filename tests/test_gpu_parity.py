@@ -55,6 +55,9 @@ RHS_CASES = [
     Config(Ns=5, Nb=1, U=0.9, EHM=True), Config(Ns=3, Nb=3, U=1.2, t2=0.2, EHM=True), Config(Ns=1, Nb=2, U=0.6, t2=0.7),
     Config(Ns=6, Nb=2, U=1.5, t2=0.3, EHM=True, vlaw="inv"), Config(Ns=4, Nb=1, U=0.0),
     Config(Ns=3, Nb=2, U=1.0, HF=True),
+    # n >= 16: the FP64 tensor-core (DMMA) halves; n = 24 and 20 pad to 32
+    Config(Ns=8, Nb=2, U=2.0, t2=0.5, EHM=True, vlaw="inv"), Config(Ns=12, Nb=2, U=1.2, t2=0.4, EHM=True),
+    Config(Ns=20, Nb=1, U=0.9, EHM=True, vlaw="inv"), Config(Ns=16, Nb=2, U=1.5, t2=0.3, EHM=True, vlaw="inv"),
 ]
 
 
