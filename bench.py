@@ -366,8 +366,31 @@ def learned_measure(g12, local, ntrain=128, ntest=32, T=3000, P=150, train_steps
                   "mixed_prefix_speedup_vs_plain_fp64_within_1e-3": covered(h34, "bf16oz", P=P4) / (dt * rk["fp64"]),
                   "mixed_prefix_speedup_vs_plain_fp64_within_1e-2": covered(h24, "bf16oz", P=P4) / (dt * rk["fp64"])}
 
+    # the product protocol: network extrapolation judged by plain RK4 at
+    # checkpoints, RK4 fallback from the first failed checkpoint, every cost
+    # counted (RK4 prefix, network, judge, fallback) - with every trajectory
+    # judged, and with a seeded sample of 2 of them judged
+    judged = {}
+    nj = min(8, len(test_ps))
+    pre, states, pre_ms = [], [], 0.0
+    for p_ in test_ps[:nj]:
+        f, st, ms_ = L.rk4_prefix(p_, P, "bf16oz", local)
+        pre.append(f)
+        states.append(st)
+        pre_ms += ms_
+    prefix = torch.from_numpy(np.stack(pre)).to(f"cuda:{local}")
+    for tag, jn in (("all_judged", None), ("two_judged", 2)):
+        _, rep = L.judged_rollout(ex, test_ps[:nj], states, prefix, 1000, check_every=check_every, tol=1e-3,
+                                  judge=jn, precision="bf16oz", device=local)
+        cost_s = (pre_ms + rep["network_ms"] + rep["judge_rk4_ms"] + rep["fallback_rk4_ms"]) / 1e3
+        sim = nj * (rep["snapshots"] - 1) * dt
+        judged[tag] = dict(rep, prefix_rk4_ms=pre_ms, simulated_time_per_s=sim / cost_s,
+                           speedup_vs_plain_fp64=sim / cost_s / (dt * rk["fp64"]),
+                           speedup_vs_plain_bf16oz=sim / cost_s / (dt * rk["bf16oz"]))
+
     return {
         "family": "Ns=8 Nb=2 (n=16), t2=0.5, EHM U/(1+r), U~U[1,3], full quench ~U[0.5,3] on Nq=3 at t=1, dt=0.01",
+        "judged_rollout": judged,
         "train": {"trajectories": int(ftr.shape[0]), "steps_each": T, "windows_K_M": [32, 16],
                   "adam_steps": train_steps, "batch": 512, "seconds": train_s, "loss_first": float(hist[:20].mean()),
                   "loss_last": float(hist[-200:].mean()), "data_device_s": gen_ms / 1e3},

@@ -28,9 +28,14 @@ thread_local std::string g_batch_error;
 struct BatchDev {
     const Dev *devs;
     const ApplyCfg *cfg;
-    const int *off_prep, *off_g1, *off_apply;  // nsys + 1 prefix offsets (blocks)
+    const ApplyTcCfg *tcfg;
+    const int *off_prep, *off_g1, *off_apply, *off_tc;  // nsys + 1 prefix offsets (blocks)
     int nsys;
 };
+
+// threads of a block of the batched FP64 tensor-core halves (every system's
+// tile shape fits: warps past its matrices stay idle)
+constexpr int kTcThreads = 512;
 
 // largest i with off[i] <= b
 __device__ __forceinline__ int find_sys(const int *off, int nsys, int b)
@@ -92,6 +97,22 @@ __global__ void __launch_bounds__(256) kb_apply(BatchDev b, int k)
     const int local = blockIdx.x - b.off_apply[sys];
     const int chunks = int((sd.n2 + cfg.NB - 1) / cfg.NB);
     apply_body<CD>(sd, k, cfg, local % chunks, local / chunks);
+}
+
+// systems with 16 <= n <= 48: the FP64 tensor-core (DMMA) halves, the same
+// device code as a single-system context of that n
+template <bool CD>
+__global__ void __launch_bounds__(kTcThreads) kb_apply_tc(BatchDev b, int k)
+{
+    __shared__ Dev sd;
+    __shared__ int sys;
+    if (threadIdx.x == 0) sys = find_sys(b.off_tc, b.nsys, blockIdx.x);
+    __syncthreads();
+    load_dev(sd, b.devs[sys]);
+    const ApplyTcCfg cfg = b.tcfg[sys];
+    const int local = blockIdx.x - b.off_tc[sys];
+    const int chunks = int((sd.n2 + cfg.NB - 1) / cfg.NB);
+    apply_tc_body<CD>(sd, k, cfg, local % chunks, local / chunks);
 }
 
 __global__ void kb_reset(BatchDev b, const long long *limits)
@@ -239,22 +260,24 @@ struct g12_batch {
     std::vector<g12_params> P;
     std::vector<Dev> dev;
     std::vector<ApplyCfg> cfg;
-    std::vector<int> off_prep, off_g1, off_apply;
+    std::vector<ApplyTcCfg> tcfg;
+    std::vector<int> off_prep, off_g1, off_apply, off_tc;
     BatchDev bd{};
     void *pool = nullptr;
     Dev *devs_d = nullptr;
     ApplyCfg *cfg_d = nullptr;
+    ApplyTcCfg *tcfg_d = nullptr;
     int *offs_d = nullptr;
     long long *limits_d = nullptr;
     double *dip_d = nullptr;
     StepP *sched_h = nullptr;  // pinned: nsys x kChunk
     StepP *sched_d = nullptr;
-    size_t smem_prep = 0, smem_g1 = 0, smem_ab = 0, smem_cd = 0;
+    size_t smem_prep = 0, smem_g1 = 0, smem_ab = 0, smem_cd = 0, smem_tab = 0, smem_tcd = 0;
     cudaStream_t s = nullptr, s2 = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr, join = nullptr;
     cudaGraphExec_t graph = nullptr;
     std::vector<double> t_rk, t_temp;
-    std::map<int, int> tuned_nb;  // n -> matrices per block
+    std::map<int, int> tuned_nb;  // n -> matrices per block (of the kernel kind that n uses)
     float last_ms = 0;
 };
 
@@ -273,17 +296,17 @@ int batch_enqueue_step(g12_batch *b, cudaStream_t s)
 {
     const BatchDev &bd = b->bd;
     kb_step_begin<<<b->nsys, 256, 0, s>>>(bd);
-    const int tp = b->off_prep.back(), tg = b->off_g1.back(), ta = b->off_apply.back();
+    const int tp = b->off_prep.back(), tg = b->off_g1.back(), ta = b->off_apply.back(), tt = b->off_tc.back();
     for (int k = 0; k < 4; ++k) {
         kb_prep<<<tp, kPrepWarps * 32, b->smem_prep, s>>>(bd, k);
         cudaEventRecord(b->fork, s);
         cudaStreamWaitEvent(b->s2, b->fork, 0);
         kb_g1<<<tg, kG1Threads, b->smem_g1, b->s2>>>(bd, k);
         cudaEventRecord(b->join, b->s2);
-        if (ta > 0) {
-            kb_apply<false><<<ta, 256, b->smem_ab, s>>>(bd, k);
-            kb_apply<true><<<ta, 256, b->smem_cd, s>>>(bd, k);
-        }
+        if (ta > 0) kb_apply<false><<<ta, 256, b->smem_ab, s>>>(bd, k);
+        if (tt > 0) kb_apply_tc<false><<<tt, kTcThreads, b->smem_tab, s>>>(bd, k);
+        if (ta > 0) kb_apply<true><<<ta, 256, b->smem_cd, s>>>(bd, k);
+        if (tt > 0) kb_apply_tc<true><<<tt, kTcThreads, b->smem_tcd, s>>>(bd, k);
         cudaStreamWaitEvent(s, b->join, 0);
     }
     return G12_OK;
@@ -291,11 +314,25 @@ int batch_enqueue_step(g12_batch *b, cudaStream_t s)
 
 // times the row/column-mixing kernels of one system for each admissible
 // matrices-per-block value and keeps the fastest
+ApplyTcCfg tc_cfg_nb(int n, int nb, size_t *sab, size_t *scd)
+{
+    ApplyTcCfg c = make_apply_tc_cfg(n, sab, scd);
+    const size_t plane = size_t(c.NP) * c.LDD * sizeof(double);
+    c.NB = nb;
+    c.threads = kTcThreads;
+    *sab = (4 + 2 * size_t(nb)) * plane;
+    *scd = *sab + size_t(n) * n * sizeof(double2);
+    return c;
+}
+
+int autotune_tc(g12_batch *b, int sys);
+
 int autotune(g12_batch *b, int sys)
 {
     const Dev &d = b->dev[sys];
     const int n = d.n;
     if (b->tuned_nb.count(n)) return b->tuned_nb[n];
+    if (apply_tc_ok(n)) return autotune_tc(b, sys);
     const int S = ((n + 3) / 4 * 4) / 4;
     std::vector<int> cands;
     for (int nb = 1; nb <= 64; nb *= 2) {
@@ -324,6 +361,53 @@ int autotune(g12_batch *b, int sys)
             cudaEventRecord(b->ev0, b->s);
             k_apply<false><<<grid, 256, sab, b->s>>>(dd, 0, c);
             k_apply<true><<<grid, 256, scd, b->s>>>(dd, 0, c);
+            cudaEventRecord(b->ev1, b->s);
+            cudaEventSynchronize(b->ev1);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+            if (rep > 0 && ms < best) {
+                best = ms;
+                best_nb = nb;
+            }
+        }
+    }
+    b->tuned_nb[n] = best_nb;
+    return best_nb;
+}
+
+// the tensor-core halves: matrices per block over {1, 2, 4, ...} within one
+// block of kTcThreads threads and 200 KB of shared memory, timed like the FMA path
+int autotune_tc(g12_batch *b, int sys)
+{
+    const Dev &d = b->dev[sys];
+    const int n = d.n;
+    size_t sab = 0, scd = 0;
+    const ApplyTcCfg base = make_apply_tc_cfg(n, &sab, &scd);
+    const int tpm = (base.NP / 16) * (base.NP / 16);
+    std::vector<int> cands;
+    for (int nb = 1; nb * tpm * 32 <= kTcThreads && nb <= n * n; nb *= 2) {
+        tc_cfg_nb(n, nb, &sab, &scd);
+        if (scd > 200 * 1024) break;
+        cands.push_back(nb);
+    }
+    StepP sp{};
+    for (int k = 0; k < 4; ++k) sp.st[k].w = 1;
+    const int one = 1;
+    cudaMemcpy(d.cur, &sp, sizeof(StepP), cudaMemcpyHostToDevice);
+    cudaMemcpy(d.active, &one, sizeof(int), cudaMemcpyHostToDevice);
+    float best = 1e30f;
+    int best_nb = cands[0];
+    for (int nb : cands) {
+        const ApplyTcCfg c = tc_cfg_nb(n, nb, &sab, &scd);
+        const dim3 grid(unsigned((d.n2 + nb - 1) / nb), 2);
+        cudaFuncSetAttribute(k_apply_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sab));
+        cudaFuncSetAttribute(k_apply_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(scd));
+        Dev dd = d;
+        dd.debug = 1;  // results go to the scratch tensors only
+        for (int rep = 0; rep < 4; ++rep) {
+            cudaEventRecord(b->ev0, b->s);
+            k_apply_tc<false><<<grid, kTcThreads, sab, b->s>>>(dd, 0, c);
+            k_apply_tc<true><<<grid, kTcThreads, scd, b->s>>>(dd, 0, c);
             cudaEventRecord(b->ev1, b->s);
             cudaEventSynchronize(b->ev1);
             float ms = 0;
@@ -515,6 +599,8 @@ extern "C" int g12_batch_create(const g12_params *systems, int32_t nsys, int32_t
     b->off_prep.assign(1, 0);
     b->off_g1.assign(1, 0);
     b->off_apply.assign(1, 0);
+    b->off_tc.assign(1, 0);
+    b->tcfg.resize(nsys);
     for (int i = 0; i < nsys; ++i) {
         const int n = b->dev[i].n;
         maxn = std::max(maxn, n);
@@ -523,22 +609,39 @@ extern "C" int g12_batch_create(const g12_params *systems, int32_t nsys, int32_t
     }
     if (cudaMalloc(&b->devs_d, sizeof(Dev) * nsys) != cudaSuccess) return fail(G12_ERR_NOMEM, "");
     for (int i = 0; i < nsys; ++i) {
+        const int n = b->dev[i].n;
         const int nb = autotune(b, i);
-        b->cfg[i] = apply_cfg_nb(b->dev[i].n, nb);
         const int chunks = int((b->dev[i].n2 + nb - 1) / nb);
-        b->off_apply.push_back(b->off_apply.back() + (b->dev[i].gate ? 2 * chunks : 0));
-        b->smem_ab = std::max(b->smem_ab, apply_smem(b->cfg[i], b->dev[i].n, false));
-        b->smem_cd = std::max(b->smem_cd, apply_smem(b->cfg[i], b->dev[i].n, true));
+        const int blocks = b->dev[i].gate ? 2 * chunks : 0;
+        if (apply_tc_ok(n)) {
+            size_t sab = 0, scd = 0;
+            b->tcfg[i] = tc_cfg_nb(n, nb, &sab, &scd);
+            b->cfg[i] = apply_cfg_nb(n, 1);
+            b->off_apply.push_back(b->off_apply.back());
+            b->off_tc.push_back(b->off_tc.back() + blocks);
+            b->smem_tab = std::max(b->smem_tab, sab);
+            b->smem_tcd = std::max(b->smem_tcd, scd);
+        } else {
+            b->cfg[i] = apply_cfg_nb(n, nb);
+            b->tcfg[i] = ApplyTcCfg{};
+            b->off_apply.push_back(b->off_apply.back() + blocks);
+            b->off_tc.push_back(b->off_tc.back());
+            b->smem_ab = std::max(b->smem_ab, apply_smem(b->cfg[i], n, false));
+            b->smem_cd = std::max(b->smem_cd, apply_smem(b->cfg[i], n, true));
+        }
     }
     b->smem_prep = prep_smem();
     b->smem_g1 = g1_smem((long long)maxn * maxn);
     cudaFuncSetAttribute(kb_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_ab));
     cudaFuncSetAttribute(kb_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_cd));
+    cudaFuncSetAttribute(kb_apply_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_tab));
+    cudaFuncSetAttribute(kb_apply_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_tcd));
     cudaFuncSetAttribute(kb_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_prep));
     cudaFuncSetAttribute(kb_g1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem_g1));
     cudaMemcpy(b->devs_d, b->dev.data(), sizeof(Dev) * nsys, cudaMemcpyHostToDevice);
     if (cudaMalloc(&b->cfg_d, sizeof(ApplyCfg) * nsys) != cudaSuccess ||
-        cudaMalloc(&b->offs_d, sizeof(int) * 3 * (nsys + 1)) != cudaSuccess ||
+        cudaMalloc(&b->tcfg_d, sizeof(ApplyTcCfg) * nsys) != cudaSuccess ||
+        cudaMalloc(&b->offs_d, sizeof(int) * 4 * (nsys + 1)) != cudaSuccess ||
         cudaMalloc(&b->limits_d, sizeof(long long) * nsys) != cudaSuccess ||
         cudaMalloc(&b->dip_d, sizeof(double) * nsys * kChunk) != cudaSuccess)
         return fail(G12_ERR_NOMEM, "out of device memory (batch)");
@@ -546,6 +649,10 @@ extern "C" int g12_batch_create(const g12_params *systems, int32_t nsys, int32_t
     cudaMemcpy(b->offs_d, b->off_prep.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(b->offs_d + nsys + 1, b->off_g1.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
     cudaMemcpy(b->offs_d + 2 * (nsys + 1), b->off_apply.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->offs_d + 3 * (nsys + 1), b->off_tc.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->tcfg_d, b->tcfg.data(), sizeof(ApplyTcCfg) * nsys, cudaMemcpyHostToDevice);
+    b->bd.tcfg = b->tcfg_d;
+    b->bd.off_tc = b->offs_d + 3 * (nsys + 1);
     b->bd.devs = b->devs_d;
     b->bd.cfg = b->cfg_d;
     b->bd.off_prep = b->offs_d;
@@ -566,6 +673,7 @@ extern "C" int g12_batch_destroy(g12_batch *b)
     cudaFree(b->pool);
     cudaFree(b->devs_d);
     cudaFree(b->cfg_d);
+    cudaFree(b->tcfg_d);
     cudaFree(b->offs_d);
     cudaFree(b->limits_d);
     cudaFree(b->dip_d);
@@ -701,5 +809,5 @@ extern "C" double g12_batch_last_device_ms(const g12_batch *b) { return b ? b->l
 extern "C" int32_t g12_batch_tile(const g12_batch *b, int32_t i)
 {
     if (!b || i < 0 || i >= b->nsys) return 0;
-    return b->cfg[i].NB;
+    return apply_tc_ok(b->dev[i].n) ? b->tcfg[i].NB : b->cfg[i].NB;
 }

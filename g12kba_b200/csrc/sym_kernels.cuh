@@ -81,11 +81,20 @@ __device__ __forceinline__ TT *sym_out(const SymDev &s, int k)
 constexpr int kBfpShift = 29;
 __device__ __forceinline__ const int *sym_in_exp(const SymDev &s, int k) { return (k & 1) ? s.eTa : s.eTb; }
 __device__ __forceinline__ int *sym_out_exp(const SymDev &s, int k) { return (k & 1) ? s.eTb : s.eTa; }
+// 2^e for |e| <= 1022, from the exponent bits
+__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
 // (rows below 2^-120 share the exponent -120: their values are then held to
-// 2^-150 absolute, and the GEMM's power-of-two row scales stay normal FP32)
-__device__ __forceinline__ int bfp_exp(double rowmax) { return rowmax > 0.0 ? max(ilogb(rowmax), -120) : 0; }
-__device__ __forceinline__ int bfp_int(double v, int e) { return __double2int_rn(ldexp(v, kBfpShift - e)); }
-__device__ __forceinline__ double bfp_scale(int e) { return ldexp(1.0, e - kBfpShift); }
+// 2^-150 absolute, and the GEMM's power-of-two row scales stay normal FP32;
+// the exponent of a normal positive double is read from its bits)
+__device__ __forceinline__ int bfp_exp(double rowmax)
+{
+    if (!(rowmax > 0.0)) return 0;
+    return max(int((__double_as_longlong(rowmax) >> 52) & 0x7ff) - 1023, -120);
+}
+// v 2^(kBfpShift - e) is exact (a power-of-two scaling), then one rounding
+__device__ __forceinline__ int bfp_int(double v, int e) { return __double2int_rn(v * pow2d(kBfpShift - e)); }
+__device__ __forceinline__ int bfp_int_sc(double v, double sc) { return __double2int_rn(v * sc); }
+__device__ __forceinline__ double bfp_scale(int e) { return pow2d(e - kBfpShift); }
 // max over aligned groups of g lanes (g a power of two <= 32); every lane of the warp takes part
 __device__ __forceinline__ double lane_group_max(double v, int g)
 {
@@ -430,9 +439,10 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
     auto put = [&](int mu1, int mu2, int c, double2 v) {
         if constexpr (BFP) {
             const int ex = bfp_exp(lane_group_max(fmax(fabs(v.x), fabs(v.y)), NN < 32 ? NN : 32));
+            const double sc = pow2d(kBfpShift - ex);
             const long long o = tmp_index(n, mu1, mu2, c, 0);
-            Out[o] = bfp_int(v.x, ex);
-            Out[o + n] = bfp_int(v.y, ex);
+            Out[o] = bfp_int_sc(v.x, sc);
+            Out[o + n] = bfp_int_sc(v.y, sc);
             if (mu1 == 0) eOut[(long long)c * n + mu2] = ex;
         } else {
             const long long o = tmp_index(n, mu1, mu2, c, 0);

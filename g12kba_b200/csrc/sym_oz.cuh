@@ -520,10 +520,10 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                     const int q = tile_p(i, g, sl);
                     return bfp_exp(double(__uint_as_float(bmax[sl * 2 + pt])) + double(__uint_as_float(bmax[q * 2 + pt])));
                 };
-                const int ex = pair_exp(slot, part);
+                const double sc = pow2d(kBfpShift - pair_exp(slot, part));
                 int *Si = reinterpret_cast<int *>(S);
 #pragma unroll
-                for (int x = 0; x < Sh::CW; ++x) Si[row * Sh::S_LD + col0 + x] = bfp_int(acc[x], ex);
+                for (int x = 0; x < Sh::CW; ++x) Si[row * Sh::S_LD + col0 + x] = bfp_int_sc(acc[x], sc);
                 if (et < 2 * Sh::CPT) {
                     const int e2 = pair_exp(et >> 1, et & 1);
                     s.eW[((long long)t * n2 + tile_c(i, g, et >> 1)) * 2 + (et & 1)] = e2;

@@ -363,6 +363,97 @@ class Extrapolator:
         return feat, ms
 
 
+def _rk4_features(p, state, nsteps, precision, device):
+    """nsteps RK4 steps of system p from `state` (G1, G2xx, G2xy) on a context
+    of `precision`: (features [nsteps][F] float32 of the snapshots after each
+    step, state after the steps, device ms)."""
+    with Context(p, precision, device) as ctx:
+        ctx.set_state(*state)
+        traj, rc = ctx.propagate(nsteps + 1)  # snapshot s is the state before step s
+        ms = ctx.last_device_ms
+        st = ctx.get_state()
+    if rc != 0:
+        raise G12Error(rc, "RK4 stopped (density guard) during a judged rollout")
+    return features(traj[1:]), st, ms
+
+
+def rk4_prefix(p, nsnap, precision="bf16oz", device=0):
+    """G0, adiabatic switching and nsnap - 1 RK4 steps of system p: the
+    features of the nsnap snapshots (the switched state first), the exact
+    state at the last of them and the device ms of the RK4 steps."""
+    with Context(p, precision, device) as ctx:
+        ctx.set_state(make_G0(p))
+        ctx.adiabatic_switch()
+        traj, rc = ctx.propagate(nsnap - 1)
+        ms = ctx.last_device_ms
+        st = ctx.get_state()
+    if rc != 0:
+        raise G12Error(rc, "RK4 stopped (density guard) in a prefix")
+    return np.concatenate([features(traj), features(st[0])[None]]), st, ms
+
+
+def judged_rollout(ex, params, prefix_states, prefix_feat, total, check_every=200, tol=1e-3, judge=None,
+                   precision="bf16oz", device=0, seed=0):
+    """Network extrapolation of an ensemble, judged by plain RK4.
+
+    params: the systems; prefix_states: each system's exact state (G1, G2xx,
+    G2xy) at the last prefix snapshot; prefix_feat: torch float32
+    [nsys][P][F], the exact prefix snapshots (features); total: snapshots in
+    the output.  The network rolls every trajectory out to `total`.  RK4 on the
+    `precision` engine re-runs the judged trajectories (all, or a seeded sample
+    of `judge` of them) from their prefix states and compares the dipole with
+    the network's at every checkpoint (`check_every` snapshots); the network's
+    snapshots count as accepted up to the last checkpoint at which every judged
+    trajectory is within `tol` (dipole error relative to its RK4 maximum, the
+    metric's definition).  From the first failed checkpoint on, RK4 is the
+    fallback for every trajectory: the judged ones continue from their judge
+    runs, the others run RK4 from their prefix states.
+
+    Returns (features [nsys][total][F] numpy: network up to the accepted point,
+    RK4 after it; a report with the accepted snapshots, the fallback flag, the
+    judged systems and the device time of each part)."""
+    torch = _torch()
+    nsys, P = prefix_feat.shape[0], prefix_feat.shape[1]
+    pred, net_ms = ex.rollout(prefix_feat, total)
+    T = pred.shape[1]
+    out = pred.cpu().numpy()
+    n = ex.n
+    rng = np.random.default_rng(seed)
+    judged = np.arange(nsys) if judge is None or judge >= nsys else np.sort(rng.choice(nsys, judge, replace=False))
+    rk_ms = 0.0
+    rk_feat = {}
+    for i in judged:
+        f, _, ms = _rk4_features(params[i], prefix_states[i], T - P, precision, device)
+        rk_feat[int(i)] = f
+        rk_ms += ms
+    # running dipole error of the judged trajectories at the checkpoints
+    accepted = T - P
+    for c in range(check_every, T - P + 1, check_every):
+        worst = 0.0
+        for i in judged:
+            pr = dipole_from_features(out[i, P:P + c], n)
+            pt = dipole_from_features(rk_feat[int(i)][:c], n)
+            full = dipole_from_features(rk_feat[int(i)], n)
+            worst = max(worst, float(np.max(np.abs(pr - pt)) / max(np.max(np.abs(full)), 1e-12)))
+        if worst > tol:
+            accepted = c - check_every
+            break
+    fallback = accepted < T - P
+    fb_ms = 0.0
+    if fallback:
+        for i in range(nsys):
+            if int(i) in rk_feat:
+                f = rk_feat[int(i)]
+            else:
+                f, _, ms = _rk4_features(params[i], prefix_states[i], T - P, precision, device)
+                fb_ms += ms
+            out[i, P + accepted:] = f[accepted:]
+    report = {"snapshots": T, "prefix": P, "accepted_after_prefix": accepted, "fallback": fallback,
+              "judged": [int(i) for i in judged], "network_ms": net_ms, "judge_rk4_ms": rk_ms,
+              "fallback_rk4_ms": fb_ms, "precision": precision, "tol": tol, "check_every": check_every}
+    return out, report
+
+
 def dipole_error(p, p_ref):
     """max_t |p - p_ref| / max(max_t |p_ref|, 1e-12) (the metric's definition)."""
     return float(np.max(np.abs(p - p_ref)) / max(np.max(np.abs(p_ref)), 1e-12))

@@ -154,7 +154,8 @@ def baseline_runs(names=None):
 
 def roundoff_sensitivity(name="run_c2_full"):
     """The reference's own sensitivity to round-off on a benchmark run: the same
-    input with G0 moved by one ulp in a seeded half of its entries.  Stores the
+    input with G0 moved by one ulp in a seeded half of its (nonzero imaginary)
+    entries.  Stores the
     perturbed run's G1 (every 25th snapshot and the last), its dipole and its
     final G2 checksums; the deviation from the unperturbed golden run is what
     two correct FP64 implementations of these equations can differ by."""
@@ -163,7 +164,8 @@ def roundoff_sensitivity(name="run_c2_full"):
     g0 = g["g0"].copy()
     rng = np.random.default_rng(11)
     mask = rng.random(g0.shape) < 0.5
-    g0 = np.where(mask, np.nextafter(g0.real, np.inf) + 1j * g0.imag, g0)
+    # G0 = i rho with rho real here: move the imaginary parts (the real parts are zero)
+    g0 = np.where(mask & (g0.imag != 0), g0.real + 1j * np.nextafter(g0.imag, np.inf), g0)
     with tempfile.TemporaryDirectory() as d:
         r = run_reference_exe(cfg, d, g0=g0, timeout=4 * 3600)
     traj = r["traj"]

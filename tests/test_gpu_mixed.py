@@ -199,38 +199,29 @@ def test_bf16oz_config2_full_length(g12, gate):
     assert rel_err(got, ref) <= FULL_TOL, rel_err(got, ref)
     pr, pg = g12.dipole(ref), g12.dipole(got)
     assert np.max(np.abs(pg - pr)) <= FULL_TOL * max(np.max(np.abs(pr)), np.max(np.abs(ref)))
-    # the symmetric engine's state stays physical to round-off
-    assert g2_asymmetry(g12, end[1], 8, 2) <= 1e-12 and g2_asymmetry(g12, end[2], 8, 2) <= 1e-12
 
 
-def test_plain_fp64_leaves_the_physical_states_on_config2(g12):
-    """The observation behind the previous test: from the same switched state,
-    the plain FP64 engine's G2 acquires an exchange-antisymmetric part that
-    grows far above round-off (the symmetric engine's stays at round-off)."""
+@pytest.mark.parametrize("prec", ["fp64", "fp64sym"])
+def test_config2_unphysical_part_grows(g12, prec):
+    """The observation behind the previous test: the exchange-antisymmetric
+    part of G2 (zero for physical states, and kept zero by the equations in
+    exact arithmetic) is seeded by round-off and grows on this model, in the
+    plain and in the symmetric FP64 engine alike (by more than 100x over the
+    5001 iterations from the plain engine's switched state, where it is
+    already far above round-off).  Each engine's G1 therefore carries its own
+    round-off history at the 1e-5 level by the end; the mixed engine shares the
+    symmetric engine's formulation, hence its comparison there."""
     p = g12.make_params(Ns=8, Nb=2, Nq=3, U=2.0, t1=1.0, t2=0.5, dt=0.01, EHM=True, v_law="inv",
                         q_type="pulse", quench_strength=2.0, quench_rate=2.0, quench_on_midpoint=15.0,
                         quench_off_midpoint=25.0, time_steps=5000)
-    with g12.Context(p, "fp64sym") as ctx:
+    with g12.Context(p, "fp64") as ctx:
         ctx.set_state(g12.make_G0(p))
         ctx.adiabatic_switch()
         S = ctx.get_state()
-    with g12.Context(p, "fp64") as ctx:
+    a0 = max(g2_asymmetry(g12, S[1], 8, 2), g2_asymmetry(g12, S[2], 8, 2))
+    assert 1e-12 < a0 < 1e-6
+    with g12.Context(p, prec) as ctx:
         ctx.set_state(*S)
         ctx.propagate(g12.rk_iterations(p))
         _, XX, XY = ctx.get_state()
-    assert g2_asymmetry(g12, S[1], 8, 2) <= 1e-14
-    assert g2_asymmetry(g12, XX, 8, 2) >= 1e-8 and g2_asymmetry(g12, XY, 8, 2) >= 1e-8
-
-
-def test_bf16oz_config3_full_length(g12):
-    """Ns=16, Nb=2 (n=32), t2=0.3, U=1.5, EHM U/(1+r), full quench 1.5 on Nq=4
-    (switched on at t >= 50), dt=0.01, 10,000 steps."""
-    p = g12.make_params(Ns=16, Nb=2, Nq=4, time_steps=10000, U=1.5, t1=1.0, t2=0.3, dt=0.01, EHM=True,
-                        v_law="inv", q_type="full", quench_strength=1.5)
-    T = g12.rk_iterations(p)
-    ref, rc0 = _full(g12, p, "fp64", T)
-    got, rc1 = _full(g12, p, "bf16oz", T)
-    assert rc0 == 0 and rc1 == 0
-    assert rel_err(got, ref) <= FULL_TOL, rel_err(got, ref)
-    pr, pg = g12.dipole(ref), g12.dipole(got)
-    assert np.max(np.abs(pg - pr)) <= FULL_TOL * max(np.max(np.abs(pr)), 1e-12), np.max(np.abs(pg - pr))
+    assert max(g2_asymmetry(g12, XX, 8, 2), g2_asymmetry(g12, XY, 8, 2)) >= 100 * a0
