@@ -558,6 +558,8 @@ def main():
         roofline = {"bound": "hbm", "kernel": top, "achieved": bytes_alg / (top_ms * 1e-3) / 1e9, "peak": hbm,
                     "unit": "GB/s", "frac": bytes_alg / (top_ms * 1e-3) / 1e9 / hbm,
                     "traffic": TOP_KERNEL_DRAM_BYTES.get(top), "algorithmic_bytes": bytes_alg,
+                    "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu "
+                                      "--set full capture of this kernel (profiles/), not measured in this run",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "source" not in peaks else "fallback"}
     else:
         flops = 32.0 * n ** 5
@@ -570,6 +572,20 @@ def main():
     step_roofline = {"bytes_per_step_fp64_state": 640.0 * n ** 4, "bytes_per_step_this_engine": mb,
                      "achieved_gbs": mb * value / world / 1e9, "frac_of_hbm": mb * value / world / 1e9 / hbm,
                      "flops_per_step": 256.0 * n ** 5, "fp64_peak_tflops": fp64_peak}
+    # the plain FP64 engine's kernels: its top kernel against the measured FP64
+    # peak (the two halves of the commutator: 16 n^5 real multiply-adds each)
+    fp_kernels = None
+    if mixed:
+        fp.set_l2_eviction(EVICT_BYTES)
+        kf = fp.kernel_times(2)
+        totf = sum(a * c for a, c in kf.values())
+        fp_kernels = {k: {"ms_per_launch": a, "launches_per_step": c, "share": a * c / totf} for k, (a, c) in kf.items()}
+        topf = max(kf, key=lambda k: kf[k][0] * kf[k][1])
+        tf = 32.0 * n ** 5 / (kf[topf][0] * 1e-3) / 1e12
+        fp_kernels["roofline"] = {"bound": "fp64", "kernel": topf, "achieved": tf, "peak": fp64_peak,
+                                  "unit": "TFLOP/s", "frac": tf / fp64_peak,
+                                  "algorithmic_flops": 32.0 * n ** 5,
+                                  "peak_source": "measured FP64 FMA probe (g12_fp64_peak_tflops) on this GPU"}
     if mixed:
         mx.close()
     fp.close()
@@ -630,7 +646,7 @@ def main():
             "status": rc, "l2_resident": {"value": world * K / (ms_res / 1e3), "unit": "steps/s",
                                           "ms_per_step": ms_res / K},
             "plain_fp64": {"value": value_fp, "unit": "steps/s", "ms_per_step": ms_fp / K,
-                                         "status": rc_fp},
+                           "status": rc_fp, "kernels": fp_kernels},
             "speedup_vs_plain_fp64": value / value_fp,
             "g1_max_rel_err_vs_fp64": g1_err,
             "fp64_symmetric": fp64sym,

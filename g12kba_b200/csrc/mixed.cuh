@@ -66,7 +66,7 @@ inline bool mixed_alloc(MixedState &m, T **p, size_t count)
     return true;
 }
 
-inline bool encode_tmp_map(CUtensorMap *map, float *base, int n, bool ints, std::string *err)
+inline bool encode_tmp_map(CUtensorMap *map, float *base, int n, std::string *err)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
@@ -85,8 +85,7 @@ inline bool encode_tmp_map(CUtensorMap *map, float *base, int n, bool ints, std:
                                    cuuint64_t(n) * n * n * n * 2 * 4};
     const cuuint32_t box[4] = {32, 1, cuuint32_t(n), 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = encode(map, ints ? CU_TENSOR_MAP_DATA_TYPE_INT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims,
-                        strides, box, estr,
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
@@ -143,9 +142,7 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
               mixed_alloc(m, &s.W, ts * size_t(2 * 2 * n4)) && mixed_alloc(m, &s.Yc, size_t(2) * s.npairs * kTB * kTB) &&
               mixed_alloc(m, &s.Ac, size_t(2) * s.npairs * kTB * kTB) && mixed_alloc(m, &s.Qt, size_t(2 * n3)) &&
               mixed_alloc(m, &s.Rtt, size_t(n2 * d.Ns)) && mixed_alloc(m, &gc, cs.size()) &&
-              mixed_alloc(m, &gp, cs.size()) && mixed_alloc(m, &pp, pairs.size()) && mixed_alloc(m, &s.err, 1) &&
-              mixed_alloc(m, &s.eTa, size_t(2 * n3)) && mixed_alloc(m, &s.eTb, size_t(2 * n3)) &&
-              mixed_alloc(m, &s.eW, size_t(2 * 2 * n2));
+              mixed_alloc(m, &gp, cs.size()) && mixed_alloc(m, &pp, pairs.size()) && mixed_alloc(m, &s.err, 1);
     if (!ok) {
         if (err) *err = "out of device memory (mixed engine)";
         return -3;
@@ -160,10 +157,7 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
                  kTB * (kTB + 1) * sizeof(double2);
     m.epi_smem = std::max(m.epi_smem, g1_smem(n2));  // G1-side blocks of k_sym_epi
     m.simt_smem = ts * ((size_t(128) * 2 * n + size_t(128) * (2 * n + 1)) * sizeof(float) + size_t(n2) * sizeof(float2));
-    if (m.oz) {
-        cudaFuncSetAttribute(k_sym_epi<16, int>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
-        cudaFuncSetAttribute(k_sym_epi<32, int>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
-    } else if (m.dbl) {
+    if (m.dbl) {
         cudaFuncSetAttribute(k_sym_epi<8, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
         cudaFuncSetAttribute(k_sym_epi<16, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
         cudaFuncSetAttribute(k_sym_epi<32, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.epi_smem));
@@ -176,8 +170,7 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
         cudaFuncSetAttribute(k_sym_gemm_simt<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(m.simt_smem));
     }
     if (m.tc) {
-        if (!encode_tmp_map(&m.map_a, s.TMPa, n, m.oz, err) || !encode_tmp_map(&m.map_b, s.TMPb, n, m.oz, err))
-            return -2;
+        if (!encode_tmp_map(&m.map_a, s.TMPa, n, err) || !encode_tmp_map(&m.map_b, s.TMPb, n, err)) return -2;
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
         m.oz2 = m.oz;
@@ -225,8 +218,7 @@ inline void mixed_free(MixedState &m)
 inline int mixed_on_state(MixedState &m, const Dev &d, cudaStream_t st)
 {
     m.s.d = d;
-    if (m.oz) k_sym_pack<int><<<dim3(m.s.npairs, 2), 256, 0, st>>>(m.s, d.Y2);
-    else if (m.dbl) k_sym_pack<double><<<dim3(m.s.npairs, 2), 256, 0, st>>>(m.s, d.Y2);
+    if (m.dbl) k_sym_pack<double><<<dim3(m.s.npairs, 2), 256, 0, st>>>(m.s, d.Y2);
     else k_sym_pack<float><<<dim3(m.s.npairs, 2), 256, 0, st>>>(m.s, d.Y2);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
@@ -298,8 +290,8 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
             SymDev sf = s;
             sf.g1x = fuse_g1 ? int((s.d.n2 + 255) / 256) : 0;
             const dim3 gf(s.npairs + sf.g1x, 2);
-            if (s.n == 32) launch_pdl(k_sym_epi<32, int>, gf, dim3(256), m.epi_smem, st, sf, k);
-            else launch_pdl(k_sym_epi<16, int>, gf, dim3(256), m.epi_smem, st, sf, k);
+            if (s.n == 32) launch_pdl(k_sym_epi<32>, gf, dim3(256), m.epi_smem, st, sf, k);
+            else launch_pdl(k_sym_epi<16>, gf, dim3(256), m.epi_smem, st, sf, k);
             return;
         }
         if (m.dbl) {
@@ -308,8 +300,8 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
             else k_sym_epi<8, double><<<g, 256, m.epi_smem, st>>>(s, k);
             return;
         }
-        if (s.n == 32 && m.oz2) launch_pdl(k_sym_epi<32, int>, g, dim3(256), m.epi_smem, st, s, k);
-        else if (s.n == 16 && m.oz2) launch_pdl(k_sym_epi<16, int>, g, dim3(256), m.epi_smem, st, s, k);
+        if (s.n == 32 && m.oz2) launch_pdl(k_sym_epi<32>, g, dim3(256), m.epi_smem, st, s, k);
+        else if (s.n == 16 && m.oz2) launch_pdl(k_sym_epi<16>, g, dim3(256), m.epi_smem, st, s, k);
         else if (s.n == 32) k_sym_epi<32><<<g, 256, m.epi_smem, st>>>(s, k);
         else if (s.n == 16) k_sym_epi<16><<<g, 256, m.epi_smem, st>>>(s, k);
         else if (s.n == 8) k_sym_epi<8><<<g, 256, m.epi_smem, st>>>(s, k);

@@ -13,8 +13,7 @@
 // e), k_sym_epi forms C = W - W^H on pairs of 32 x 32 tiles (R, C) / (C, R) and
 // fuses the rest of the stage (Psi, Pi, K2, RK4 bookkeeping) like k_apply<true>.
 //
-// Storage (per tensor t = xx, xy; TT = int block floating point in BF16OZ,
-// FP32 in the other mixed modes, FP64 in FP64SYM):
+// Storage (per tensor t = xx, xy; TT = FP32 in the mixed modes, FP64 in FP64SYM):
 //   TMP  (TT, GEMM input):    ((mu2*n^2 + c)*2 + part)*n + mu1
 //   W    (TT):                (c*2 + part)*n^2 + r
 //   Yc, Ac (FP64 complex):    Hermitian-compressed state and RK4 sum: for each
@@ -24,8 +23,6 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
-
-#include <type_traits>
 
 #include "fp64_kernels.cuh"
 
@@ -39,10 +36,8 @@ struct SymDev {
     int gemm_tiles;         // GEMM tiles per tensor
     int nblk, npairs;       // epilogue blocks per edge, tile pairs per tensor
     long long n4;
-    float *TMPa, *TMPb;     // 2 tensors each (storage type of the mode, see below)
+    float *TMPa, *TMPb;     // 2 tensors each
     float *W;               // 2 tensors
-    int *eTa, *eTb;         // BFP row exponents of TMPa / TMPb: [t][c][mu2]
-    int *eW;                // BFP row exponents of W: [t][c][part]
     double2 *Yc, *Ac;       // 2 tensors x npairs x kTB^2
     double2 *Qt, *Rtt;      // transposed copies of Q ([r][b][a]) and Rt ([s][b][a])
     const int *gemm_c;      // [gemm_tiles][cpt] c values
@@ -72,41 +67,10 @@ __device__ __forceinline__ TT *sym_out(const SymDev &s, int k)
     return reinterpret_cast<TT *>((k & 1) ? s.TMPb : s.TMPa);
 }
 
-// Block floating point (the BF16OZ mode, storage type int): a row of values
-// v shares the exponent e = ilogb(max |v|) and each value is the integer
-// x = rint(v 2^(kBfpShift - e)), |x| <= 2^30, so v = x 2^(e - kBfpShift) with an
-// error of at most 2^(e - kBfpShift - 1), i.e. 2^-31 of the row maximum.
-// Rows: TMP row (t, mu2, c) over (part, mu1) (one A row of the W contraction),
-// exponents stored [t][c][mu2]; W row (t, c, part) over r, exponents [t][c][part].
-constexpr int kBfpShift = 29;
-__device__ __forceinline__ const int *sym_in_exp(const SymDev &s, int k) { return (k & 1) ? s.eTa : s.eTb; }
-__device__ __forceinline__ int *sym_out_exp(const SymDev &s, int k) { return (k & 1) ? s.eTb : s.eTa; }
-// 2^e for |e| <= 1022, from the exponent bits
-__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(1023 + e) << 52); }
-// (rows below 2^-120 share the exponent -120: their values are then held to
-// 2^-150 absolute, and the GEMM's power-of-two row scales stay normal FP32;
-// the exponent of a normal positive double is read from its bits)
-__device__ __forceinline__ int bfp_exp(double rowmax)
-{
-    if (!(rowmax > 0.0)) return 0;
-    return max(int((__double_as_longlong(rowmax) >> 52) & 0x7ff) - 1023, -120);
-}
-// v 2^(kBfpShift - e) is exact (a power-of-two scaling), then one rounding
-__device__ __forceinline__ int bfp_int(double v, int e) { return __double2int_rn(v * pow2d(kBfpShift - e)); }
-__device__ __forceinline__ int bfp_int_sc(double v, double sc) { return __double2int_rn(v * sc); }
-__device__ __forceinline__ double bfp_scale(int e) { return pow2d(e - kBfpShift); }
-// max over aligned groups of g lanes (g a power of two <= 32); every lane of the warp takes part
-__device__ __forceinline__ double lane_group_max(double v, int g)
-{
-    for (int o = g / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
 // complex pair of the storage type
 template <typename TT> struct Cx2;
 template <> struct Cx2<float> { using T = float2; };
 template <> struct Cx2<double> { using T = double2; };
-template <> struct Cx2<int> { using T = int2; };
 template <typename TT>
 __device__ __forceinline__ typename Cx2<TT>::T mk2(TT a, TT b)
 {
@@ -182,7 +146,6 @@ template <int NN, typename TT = float>
 __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
 {
     using T2 = typename Cx2<TT>::T;
-    constexpr bool BFP = std::is_same<TT, int>::value;
     if (!*s.d.active) return;
     const Dev &d = s.d;
     if (blockIdx.x >= s.npairs) {
@@ -216,34 +179,14 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
     T2 *Wcr = Wrc + kTB * (kTB + 1);                   // [r_l][c_l] = W[C0+c_l][R0+r_l]
     double2 *Ks = reinterpret_cast<double2 *>(Wcr + kTB * (kTB + 1));  // [c_l][r_l] tmp_next (or K), rows of KLD
     __shared__ int site[NN];
-    // BFP: scales of the W rows C0 + l (Wrc) and R0 + l (Wcr), (part 0, part 1)
-    __shared__ double2 scC[BFP ? kTB : 1], scR[BFP ? kTB : 1];
     const TT *Wg = reinterpret_cast<const TT *>(s.W) + t * 2 * s.n4;
     const double2 *G1 = (k & 1) ? d.G1t1 : d.G1t0;
     if (threadIdx.x < NN) site[threadIdx.x] = threadIdx.x % Ns;
-    auto w_of = [&](T2 w1, T2 w2, int rl, int cl) -> double2 {
-        // C = W - W^H at (R0 + rl, C0 + cl): w1 = W[R0+rl][C0+cl], w2 = W[C0+cl][R0+rl]
-        if constexpr (BFP) {
-            const double2 a = scC[cl], b = scR[rl];
-            return make_double2(double(w1.x) * a.x - double(w2.x) * b.x, double(w1.y) * a.y + double(w2.y) * b.y);
-        } else {
-            return make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
-        }
-    };
 #pragma unroll 4
     for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[(x / n) * GLD + x % n] = G1[x];
     // W comes from the GEMM launched just before this kernel (G1 and the tables
     // of k_prep were complete before it started)
     grid_dep_wait();
-    if constexpr (BFP) {
-        if (threadIdx.x < 2 * kTB) {
-            const int l = threadIdx.x % kTB, row = (threadIdx.x < kTB) ? C0 + l : R0 + l;
-            const int *eW = s.eW + ((long long)t * n2 + row) * 2;
-            const double2 v = make_double2(bfp_scale(eW[0]), bfp_scale(eW[1]));
-            if (threadIdx.x < kTB) scC[l] = v;
-            else scR[l] = v;
-        }
-    }
 #pragma unroll
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
@@ -313,7 +256,9 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
             const int cl = (threadIdx.x >> 5) + 8 * j;
             const int e = cl * kTB + rl;  // = threadIdx.x + 256 j
             const int nu1 = c0 + cl;
-            const double2 C = w_of(Wrc[cl * (kTB + 1) + rl], Wcr[rl * (kTB + 1) + cl], rl, cl);
+            const T2 w1 = Wrc[cl * (kTB + 1) + rl];
+            const T2 w2 = Wcr[rl * (kTB + 1) + cl];
+            const double2 C = make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
             const double2 g11 = Gs[mu1 * GLD + nu1];
             const double2 g1122 = c_mul(g11, g22);
             const double wd = wa - wb[cl];
@@ -355,8 +300,10 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
         const int rl = e % kTB, cl = e / kTB;
         const int r = R0 + rl, c = C0 + cl;
         const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
+        const T2 w1 = Wrc[cl * (kTB + 1) + rl];
         // W[c][r] = Wcr at (row offset cl in block C -> index rl' = cl, col r -> cl' = rl)
-        const double2 C = w_of(Wrc[cl * (kTB + 1) + rl], Wcr[rl * (kTB + 1) + cl], rl, cl);
+        const T2 w2 = Wcr[rl * (kTB + 1) + cl];
+        const double2 C = make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
         const int si = site[mu1], sj = site[mu2], sk = site[nu1], sl = site[nu2];
         const double2 g11 = Gs[mu1 * GLD + nu1], g22 = Gs[mu2 * GLD + nu2];
         const double wd = (U * double(si == sj) + vdist(si, sj)) - (U * double(sk == sl) + vdist(sk, sl));
@@ -432,36 +379,24 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
     }
     __syncthreads();
     TT *Out = sym_out<TT>(s, k) + t * 2 * s.n4;
-    int *eOut = BFP ? sym_out_exp(s, k) + (long long)t * n * n2 : nullptr;
-    // next-stage input of tile (R, C) and, off the diagonal, tile (C, R) =
-    // conj of its transpose.  The lanes of a warp hold whole A rows (mu2, c)
-    // over mu1 (NN <= 32), so BFP row exponents are lane-group maxima.
-    auto put = [&](int mu1, int mu2, int c, double2 v) {
-        if constexpr (BFP) {
-            const int ex = bfp_exp(lane_group_max(fmax(fabs(v.x), fabs(v.y)), NN < 32 ? NN : 32));
-            const double sc = pow2d(kBfpShift - ex);
-            const long long o = tmp_index(n, mu1, mu2, c, 0);
-            Out[o] = bfp_int_sc(v.x, sc);
-            Out[o + n] = bfp_int_sc(v.y, sc);
-            if (mu1 == 0) eOut[(long long)c * n + mu2] = ex;
-        } else {
-            const long long o = tmp_index(n, mu1, mu2, c, 0);
-            Out[o] = TT(v.x);
-            Out[o + n] = TT(v.y);
-        }
-    };
     // tile (R, C): fastest index mu1 = r % n follows rl
     for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
         const int rl = e % kTB, cl = e / kTB;
         const int r = R0 + rl, c = C0 + cl;
-        put(r % n, r / n, c, Ks[cl * KLD + rl]);
+        const double2 v = Ks[cl * KLD + rl];
+        const long long o = tmp_index(n, r % n, r / n, c, 0);
+        Out[o] = TT(v.x);
+        Out[o + n] = TT(v.y);
     }
     if (!diag) {
         // tile (C, R): element (c, r) = conj(v); fastest index nu1 = c % n follows cl
         for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
             const int cl = e % kTB, rl = e / kTB;
             const int r = R0 + rl, c = C0 + cl;
-            put(c % n, c / n, r, c_conj(Ks[cl * KLD + rl]));
+            const double2 v = Ks[cl * KLD + rl];
+            const long long o = tmp_index(n, c % n, c / n, r, 0);
+            Out[o] = TT(v.x);
+            Out[o + n] = TT(-v.y);
         }
     }
 }
@@ -480,54 +415,22 @@ __global__ void k_sym_pack(SymDev s, const double2 *Yfull)
     double2 *Yc = s.Yc + ((long long)t * s.npairs + p) * kTB * kTB;
     TT *Out = reinterpret_cast<TT *>(s.TMPb) + t * 2 * s.n4;
     double2 *Dt = s.d.D + t * n3;
-    if constexpr (std::is_same<TT, int>::value) {
-        // BFP stage input: the lanes of a warp hold whole A rows over mu1
-        // (n in {16, 32}), tile (R, C) first, then its conjugate transpose
-        int *eOut = s.eTb + (long long)t * n * n2;
-        for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
-            const int rl = e % kTB, cl = e / kTB;
-            const int r = R0 + rl, c = C0 + cl;
-            const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
-            const double2 v = Y[(long long)c + n2 * mu1 + n3 * mu2];
-            Yc[e] = v;
-            if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = v;
-            if (rc.x != rc.y && nu2 == mu2) Dt[((long long)nu1 * n + mu1) * n + nu2] = c_conj(v);
-            const int ex = bfp_exp(lane_group_max(fmax(fabs(v.x), fabs(v.y)), n < 32 ? n : 32));
-            const long long o = tmp_index(n, mu1, mu2, c, 0);
-            Out[o] = bfp_int(v.x, ex);
-            Out[o + n] = bfp_int(v.y, ex);
-            if (mu1 == 0) eOut[(long long)c * n + mu2] = ex;
-        }
-        if (rc.x != rc.y)
-            for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
-                const int cl = e % kTB, rl = e / kTB;
-                const int r = R0 + rl, c = C0 + cl;
-                const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
-                const double2 v = c_conj(Y[(long long)c + n2 * mu1 + n3 * mu2]);
-                const int ex = bfp_exp(lane_group_max(fmax(fabs(v.x), fabs(v.y)), n < 32 ? n : 32));
-                const long long o = tmp_index(n, nu1, nu2, r, 0);
-                Out[o] = bfp_int(v.x, ex);
-                Out[o + n] = bfp_int(v.y, ex);
-                if (nu1 == 0) eOut[(long long)r * n + nu2] = ex;
-            }
-    } else {
-        for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
-            const int rl = e % kTB, cl = e / kTB;
-            const int r = R0 + rl, c = C0 + cl;
-            const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
-            // device orbital layout: x = nu1 + n*nu2 + n^2*mu1 + n^3*mu2
-            const double2 v = Y[(long long)c + n2 * mu1 + n3 * mu2];
-            Yc[e] = v;
-            long long o = tmp_index(n, mu1, mu2, c, 0);
+    for (int e = threadIdx.x; e < kTB * kTB; e += blockDim.x) {
+        const int rl = e % kTB, cl = e / kTB;
+        const int r = R0 + rl, c = C0 + cl;
+        const int mu1 = r % n, mu2 = r / n, nu1 = c % n, nu2 = c / n;
+        // device orbital layout: x = nu1 + n*nu2 + n^2*mu1 + n^3*mu2
+        const double2 v = Y[(long long)c + n2 * mu1 + n3 * mu2];
+        Yc[e] = v;
+        long long o = tmp_index(n, mu1, mu2, c, 0);
+        Out[o] = TT(v.x);
+        Out[o + n] = TT(v.y);
+        if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = v;
+        if (rc.x != rc.y) {
+            o = tmp_index(n, nu1, nu2, r, 0);
             Out[o] = TT(v.x);
-            Out[o + n] = TT(v.y);
-            if (mu2 == nu2) Dt[((long long)mu1 * n + nu1) * n + mu2] = v;
-            if (rc.x != rc.y) {
-                o = tmp_index(n, nu1, nu2, r, 0);
-                Out[o] = TT(v.x);
-                Out[o + n] = TT(-v.y);
-                if (nu2 == mu2) Dt[((long long)nu1 * n + mu1) * n + nu2] = c_conj(v);
-            }
+            Out[o + n] = TT(-v.y);
+            if (nu2 == mu2) Dt[((long long)nu1 * n + mu1) * n + nu2] = c_conj(v);
         }
     }
 }

@@ -38,6 +38,21 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t
         : "memory");
 }
 
+// Round to the nearest integer (ties to even) for |x| < 2^22 by adding and
+// removing 1.5 * 2^23: the sum's rounding discards exactly the fraction.  Two
+// full-rate FP32 operations instead of the conversion pipe's rounding.
+__device__ __forceinline__ float rint_small(float x)
+{
+    return __fadd_rn(__fadd_rn(x, 12582912.0f), -12582912.0f);
+}
+
+// rint_small(a * b) with one rounding (the product of a and a power of two b is exact)
+__device__ __forceinline__ float rint_small_mul(float a, float b)
+{
+    return __fadd_rn(__fmaf_rn(a, b, 12582912.0f), -12582912.0f);
+}
+
+
 // two small integers (|d| <= 256, exact in bf16) -> packed bf16x2 (a in the low
 // half): the bf16 of such a value is the upper half of its FP32 bit pattern
 __device__ __forceinline__ uint32_t bf16x2_of_ints(float a, float b)
@@ -138,56 +153,41 @@ __device__ __forceinline__ void named_sync(int id, int nthreads)
 
 // Warp-specialised, persistent digit GEMM (same tiles as k_sym_gemm_tc) with
 // four 8-bit digits per operand:
-//   a = 2^(e - 6) (d0 + d1 2^-8 + d2 2^-16 + d3 2^-24),  |d_i| <= 128 (exact in bf16).
-// The stage input arrives in block floating point (sym_kernels.cuh: one
-// exponent per A row, 30-bit integers, formed from the FP64 stage input by the
-// previous epilogue), so the digits are an exact integer split of each value
-// and the operand carries 2^-31 of its row maximum.  The digits of h come from
-// k_prep (h_digits, a 2^(30 - e) scaling of the FP64 entries split by
-// round-to-nearest: 2^-32 of the row maximum).
+//   a = 2^(e - 6) (d0 + d1 2^-8 + d2 2^-16 + d3 2^-24),  |d_i| <= 128 (exact in bf16),
+// obtained by successive round-to-nearest of a 2^(30 - e) (e = exponent of the
+// row maximum): every FP32 value within 2^8 of its row maximum is represented
+// exactly, the rest to 2^-32 of the maximum.  (Three digits, with a remainder of
+// 2^-23 of the row maximum, let G1 drift to 4e-6 over 10,000 steps at n = 32.)
 // Products with digit levels i + j = L <= 3 accumulate in TMEM accumulator L:
 // |sum| <= 4 * K * 128 * 128 <= 2^22 < 2^24, exact in FP32 whatever the
-// accumulator's rounding; T1 = 2^(e_m - 6) 2^(e_j - 6) sum_L 2^(-8L) P_L,
-// combined exactly in FP64.  W = T1 + e(T1) leaves in block floating point:
-// one exponent per W row pair (c, cbar) and part, T1 staged as integers on
-// that grid, so W is an exact integer sum (2^-30 of the pair's maximum).
+// accumulator's rounding; T1 = 2^(e_m - 6) 2^(e_j - 6) sum_L 2^(-8L) P_L.
 // Roles (26 warps at n = 32, 18 at n = 16):
-//   warp 0      TMA producer: A tiles and their row exponents into a 2-stage
-//               ring (starts as soon as the barriers exist)
+//   warp 0      TMA producer: FP32 A tiles into a 2-stage ring (starts as soon
+//               as the barriers exist)
 //   warp 1      one thread issues the 10 digit products per tile into one of
 //               two TMEM accumulator sets
-//   warps 2-9   digit split, two threads per A row (4 bf16 digit rows)
+//   warps 2-9   digit split, two threads per A row (row max, exponent, 4 bf16
+//               digit rows)
 //   warps 10-  epilogue (16 warps at n = 32, 8 at n = 16), four per column
-//               group, one per TMEM lane quadrant: TMEM -> FP64 combination ->
-//               block maxima -> integer staging -> W = T1 + e(T1)
+//               group, one per TMEM lane quadrant: TMEM -> FP32 combination ->
+//               staging -> W = T1 + e(T1)
 // so the loads of tile i+2, the digits and products of tile i+1 and the
-// epilogue of tile i overlap.  Every wait is bounded.
+// epilogue of tile i overlap.  The digits of h come from k_prep
+// (h_digits).  Every wait is bounded.
 constexpr int kOz2Digits = 4;     // digits per operand = accumulation levels
 constexpr int kOz2ListTiles = 8;  // tiles per CTA whose c / partner lists are staged in shared memory
 
-// signed 8-bit digits of a BFP integer (|x| <= 2^30): x = d0 2^24 + d1 2^16 +
-// d2 2^8 + d3 with d1..d3 in [-128, 127] and |d0| <= 64, all exact integer steps
-__device__ __forceinline__ void oz2_digits_int(int x, float (&d)[kOz2Digits])
+// digits of x (|x| < 2^31): x = d0 2^24 + d1 2^16 + d2 2^8 + d3 + r, every step exact
+__device__ __forceinline__ void oz2_digits(float x, float (&d)[kOz2Digits])
 {
-    const int d3 = int((signed char)(x & 255));
-    int y = (x - d3) >> 8;
-    const int d2 = int((signed char)(y & 255));
-    y = (y - d2) >> 8;
-    const int d1 = int((signed char)(y & 255));
-    y = (y - d1) >> 8;
-    d[0] = float(y);
-    d[1] = float(d1);
-    d[2] = float(d2);
-    d[3] = float(d3);
-}
-
-// bulk copy global -> shared (no multicast), completion on an mbarrier
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
+    float r = x;
+    d[0] = rint_small_mul(r, 0x1p-24f);
+    r = __fmaf_rn(-d[0], 0x1p24f, r);
+    d[1] = rint_small_mul(r, 0x1p-16f);
+    r = __fmaf_rn(-d[1], 0x1p16f, r);
+    d[2] = rint_small_mul(r, 0x1p-8f);
+    r = __fmaf_rn(-d[2], 0x1p8f, r);
+    d[3] = rint_small(r);
 }
 
 template <int NN>
@@ -217,9 +217,7 @@ struct Oz2Shape {
     static constexpr int OFF_S = OFF_B + kOz2Digits * B_BYTES;       // 128 x S_LD floats
     static constexpr int OFF_E = OFF_S + 128 * S_LD * 4;             // eA[4][128], sB[N]
     static constexpr int OFF_L = OFF_E + 4 * 128 * 4 + N * 4;        // tile lists: c, partner
-    static constexpr int OFF_X = OFF_L + 2 * kOz2ListTiles * CPT * 4; // 2 stages of 128 row exponents
-    static constexpr int OFF_M = OFF_X + 2 * 128 * 4;                 // block maxima [CPT][2]
-    static constexpr int OFF_BAR = OFF_M + 2 * CPT * 4 + 2 * CPT * 4;
+    static constexpr int OFF_BAR = OFF_L + 2 * kOz2ListTiles * CPT * 4;
     static constexpr int SMEM = OFF_BAR + 16 * 8 + 1024;
     static_assert(kOz2Digits * N <= ACC, "accumulator set");
     static_assert(SMEM <= 227 * 1024, "shared memory");
@@ -240,8 +238,6 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
     float *sB = reinterpret_cast<float *>(eA + 4 * 128);         // [N]
     int *lc = reinterpret_cast<int *>(sm + Sh::OFF_L);           // [kOz2ListTiles][CPT] c values
     int *lp = lc + kOz2ListTiles * Sh::CPT;                      // partner slots
-    int *Xe = reinterpret_cast<int *>(sm + Sh::OFF_X);           // [2][128] BFP row exponents of the A stages
-    unsigned *bmax = reinterpret_cast<unsigned *>(sm + Sh::OFF_M);  // [CPT][2] max |T1| (float bits, rounded up)
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + Sh::OFF_BAR);
     uint64_t *full_a = bar, *empty_a = bar + 2, *dig_full = bar + 4, *dig_empty = bar + 6, *acc_full = bar + 8,
              *acc_empty = bar + 10;
@@ -270,7 +266,6 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
         mbar_init(b_ready, Sh::EPI);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int x = tid; x < 2 * Sh::CPT; x += blockDim.x) bmax[x] = 0u;
     // c values and partner slots of this CTA's first tiles (independent loads)
     for (int x = tid; x < min(my_tiles, kOz2ListTiles) * Sh::CPT; x += blockDim.x) {
         const int g = (blockIdx.x + (x / Sh::CPT) * gridDim.x) % s.gemm_tiles;
@@ -305,15 +300,12 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                     ok = false;
                     break;
                 }
-                mbar_expect_tx(&full_a[sa], Sh::A_STAGE + Sh::CPT * NN * 4);
-                const int *eTin = sym_in_exp(s, k) + (long long)t * NN * n2;
+                mbar_expect_tx(&full_a[sa], Sh::A_STAGE);
                 for (int slot = 0; slot < Sh::CPT; ++slot) {
                     const int c = tile_c(i, g, slot);
                     for (int kb = 0; kb < Sh::KB; ++kb)
                         tma_load_4d(As + sa * Sh::A_STAGE + kb * 128 * 128 + slot * NN * 128, &tmap, &full_a[sa],
                                     kb * 32, c, 0, t);
-                    // the BFP exponents of the slot's NN rows (mu2 = 0..NN-1), contiguous ([t][c][mu2])
-                    bulk_load(Xe + sa * 128 + slot * NN, eTin + (long long)c * NN, NN * 4, &full_a[sa]);
                 }
                 issued = i + 1;
             }
@@ -384,7 +376,7 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                     ok = false;
                     break;
                 }
-                int v[HF];
+                float v[HF];
                 const unsigned char *row = As + sa * Sh::A_STAGE + m * 128;
                 // n = 32: the two halves of a row sit at the same chunk of two
                 // 128-byte boxes; the second half reads its chunks in the order
@@ -396,7 +388,7 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                 for (int q4 = 0; q4 < HF / 4; ++q4) {
                     const int f = half * HF + 4 * (q4 ^ hx);     // first FP32 index of this 16-byte chunk
                     const int kb = f >> 5, j = (f & 31) >> 2;
-                    const int4 q = *reinterpret_cast<const int4 *>(row + kb * 128 * 128 + ((j ^ sw) << 4));
+                    const float4 q = *reinterpret_cast<const float4 *>(row + kb * 128 * 128 + ((j ^ sw) << 4));
                     v[4 * q4 + 0] = q.x;
                     v[4 * q4 + 1] = q.y;
                     v[4 * q4 + 2] = q.z;
@@ -406,15 +398,20 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                     if (half) {
 #pragma unroll
                         for (int x = 0; x < HF / 2; ++x) {
-                            const int tmp = v[x];
+                            const float tmp = v[x];
                             v[x] = v[x + HF / 2];
                             v[x + HF / 2] = tmp;
                         }
                     }
                 }
-                // a = x 2^(e - kBfpShift) = 2^(e + 1 - 6) (d0 + d1 2^-8 + d2 2^-16 + d3 2^-24)
-                if (half == 0) eA[(i & 3) * 128 + m] = Xe[sa * 128 + m] + 1;
                 mbar_arrive(&empty_a[sa]);
+                float mx = 0.f;
+#pragma unroll
+                for (int x = 0; x < HF; ++x) mx = fmaxf(mx, fabsf(v[x]));
+                mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+                const int e = (mx > 0.f) ? max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, -100) : 0;
+                if (half == 0) eA[(i & 3) * 128 + m] = e;
+                const float sc = pow2f(30 - e);
                 unsigned char *Dst = Ds + db * Sh::D_SET + m * 128;
 #pragma unroll
                 for (int hc = 0; hc < HC; ++hc) {
@@ -423,8 +420,8 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
 #pragma unroll
                     for (int pr = 0; pr < 4; ++pr) {
                         float d0[kOz2Digits], d1[kOz2Digits];
-                        oz2_digits_int(v[hc * 8 + 2 * pr], d0);
-                        oz2_digits_int(v[hc * 8 + 2 * pr + 1], d1);
+                        oz2_digits(v[hc * 8 + 2 * pr] * sc, d0);
+                        oz2_digits(v[hc * 8 + 2 * pr + 1] * sc, d1);
 #pragma unroll
                         for (int q = 0; q < kOz2Digits; ++q) w4[q][pr] = bf16x2_of_ints(d0[q], d1[q]);
                     }
@@ -475,13 +472,13 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                     break;
                 }
                 tc_fence_after();
-                const double sa = double(pow2f(eA[(i & 3) * 128 + row] - 6));
+                const float sa = pow2f(eA[(i & 3) * 128 + row] - 6);
                 const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * Sh::ACC + col0;
-                double acc[Sh::CW];
+                float acc[Sh::CW];
 #pragma unroll
-                for (int x = 0; x < Sh::CW; ++x) acc[x] = 0.0;
-                // sum_L 2^(-8L) P_L, smallest level first, in FP64: every P_L is an
-                // integer below 2^24, so the sum (46 significant bits) is exact
+                for (int x = 0; x < Sh::CW; ++x) acc[x] = 0.f;
+                // sum_L 2^(-8L) P_L, smallest level first (FP32, round to nearest);
+                // LB levels loaded per wait
 #pragma unroll
                 for (int L0 = kOz2Digits - 1; L0 >= 0; L0 -= LB) {
                     float wv[LB][Sh::CW];
@@ -495,52 +492,25 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                     for (int l = 0; l < LB; ++l)
                         if (L0 - l >= 0) {
 #pragma unroll
-                            for (int x = 0; x < Sh::CW; ++x) acc[x] = fma(acc[x], 0x1p-8, double(wv[l][x]));
+                            for (int x = 0; x < Sh::CW; ++x) acc[x] = fmaf(acc[x], 0x1p-8f, wv[l][x]);
                         }
                 }
-                // the accumulator set is free once its values are in registers
+#pragma unroll
+                for (int x = 0; x < Sh::CW; ++x) S[row * Sh::S_LD + col0 + x] = acc[x] * sa * sB[col0 + x];
                 tc_fence_before();
                 mbar_arrive(&acc_empty[b]);
-                // T1 (exact power-of-two scaling) and its maximum per (slot, part):
-                // the rows of a slot are NN consecutive lanes, the warp's columns one part
-                const int slot = row / NN, part = col0 / NN;
-                double mx = 0.0;
-#pragma unroll
-                for (int x = 0; x < Sh::CW; ++x) {
-                    acc[x] *= sa * double(sB[col0 + x]);
-                    mx = fmax(mx, fabs(acc[x]));
-                }
-                mx = lane_group_max(mx, NN);
-                if ((lane & (NN - 1)) == 0) atomicMax(&bmax[slot * 2 + part], __float_as_uint(__double2float_ru(mx)));
                 named_sync(1, Sh::EPI);
-                // W rows c and cbar (an exchange pair) hold the same values: one BFP
-                // exponent per pair and part, from the bound |W| <= max|T1(c)| + max|T1(cbar)|;
-                // T1 is staged as integers on that grid, so W = S1 + S2 is an exact integer sum
-                auto pair_exp = [&](int sl, int pt) {
-                    const int q = tile_p(i, g, sl);
-                    return bfp_exp(double(__uint_as_float(bmax[sl * 2 + pt])) + double(__uint_as_float(bmax[q * 2 + pt])));
-                };
-                const double sc = pow2d(kBfpShift - pair_exp(slot, part));
-                int *Si = reinterpret_cast<int *>(S);
-#pragma unroll
-                for (int x = 0; x < Sh::CW; ++x) Si[row * Sh::S_LD + col0 + x] = bfp_int_sc(acc[x], sc);
-                if (et < 2 * Sh::CPT) {
-                    const int e2 = pair_exp(et >> 1, et & 1);
-                    s.eW[((long long)t * n2 + tile_c(i, g, et >> 1)) * 2 + (et & 1)] = e2;
-                }
-                named_sync(1, Sh::EPI);
-                if (et < 2 * Sh::CPT) bmax[et] = 0u;  // read above; next written after the next tile's first barrier
-                int *Wg = reinterpret_cast<int *>(s.W) + t * 2 * s.n4;
+                float *Wg = s.W + t * 2 * s.n4;
 #pragma unroll 2
                 for (int sp = 0; sp < Sh::CPT * 2; ++sp) {
-                    const int sl = sp >> 1, pt = sp & 1;
-                    const int ps = tile_p(i, g, sl);
-                    int *Wrow = Wg + ((long long)tile_c(i, g, sl) * 2 + pt) * n2;
+                    const int slot = sp >> 1, part = sp & 1;
+                    const int ps = tile_p(i, g, slot);
+                    float *Wrow = Wg + ((long long)tile_c(i, g, slot) * 2 + part) * n2;
 #pragma unroll
                     for (int r = et; r < NN * NN; r += Sh::EPI) {
                         const int mu1 = r % NN, mu2 = r / NN;
-                        Wrow[r] = Si[(sl * NN + mu2) * Sh::S_LD + pt * NN + mu1] +
-                                  Si[(ps * NN + mu1) * Sh::S_LD + pt * NN + mu2];
+                        Wrow[r] = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] +
+                                  S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
                     }
                 }
                 named_sync(1, Sh::EPI);
