@@ -5,7 +5,7 @@
 // reference's formats and stdout lines.
 //
 // Extension input keys (ignored by the reference): precision (fp64 | bf16oz |
-// tf32x3 | tf32x6 | fp32), device, G0_file (n*n complex128 binary replacing make_G0), plus
+// tf32x3 | tf32x6 | fp32 | fp64sym), device, G0_file (n*n complex128 binary replacing make_G0), plus
 // V_law, quench_gate and AS_dt handled by g12_read_input.
 #include "g12kba.h"
 
@@ -48,6 +48,7 @@ int main(int argc, char **argv)
     else if (pv == "tf32x6") prec = G12_PREC_TF32X6;
     else if (pv == "bf16oz") prec = G12_PREC_BF16OZ;
     else if (pv == "fp32") prec = G12_PREC_FP32;
+    else if (pv == "fp64sym") prec = G12_PREC_FP64SYM;
     int device = 0;
     std::string dv = ext_value("device");
     if (!dv.empty()) device = std::atoi(dv.c_str());
