@@ -317,7 +317,7 @@ int batch_enqueue_step(g12_batch *b, cudaStream_t s)
 ApplyTcCfg tc_cfg_nb(int n, int nb, size_t *sab, size_t *scd)
 {
     ApplyTcCfg c = make_apply_tc_cfg(n, sab, scd);
-    const size_t plane = size_t(c.NP) * c.LDD * sizeof(double);
+    const size_t plane = size_t(apply_tc_plane(c.NP, c.LDD)) * sizeof(double);
     c.NB = nb;
     c.threads = kTcThreads;
     *sab = (4 + 2 * size_t(nb)) * plane;

@@ -234,7 +234,10 @@ void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
         k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, s>>>(d, k);
         if (ctx->prec != G12_PREC_FP64 && d.gate && mixed_fuses_g1(ctx->mixed)) {
             // digit GEMM, then the epilogue with the G1 side as extra blocks of
-            // its launch (two launches per stage after k_prep)
+            // its launch (two launches per stage after k_prep).  (Running
+            // k_prep's table blocks on a side stream beside the GEMM was
+            // measured slower: the join before the epilogue costs it its
+            // programmatic launch.)
             mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, 0, s);
             mixed_enqueue_kind(ctx->mixed, d, k, ctx->prec, 1, s, true);
             continue;

@@ -249,27 +249,44 @@ __device__ __forceinline__ void h_digits(const Dev &d, double2 hv, int x)
     }
 }
 
+// h (HF.h:57-104), one entry per thread, and its digits for the tensor cores;
+// hb: block index among the h blocks
+__device__ __forceinline__ void prep_h_part(const Dev &d, int k, int hb)
+{
+    if (!*d.active) return;
+    const StageP st = d.cur->st[k];
+    const int n = d.n;
+    const long long n2 = (long long)n * n;
+    const double2 *__restrict__ G = g1_stage(d, k);
+    extern __shared__ double2 sm_h[];
+    for (int p = threadIdx.x; p < n; p += blockDim.x) sm_h[p] = G[(long long)p * n + p];
+    __syncthreads();
+    const long long x = (long long)hb * blockDim.x + threadIdx.x;
+    double2 hv = make_double2(0.0, 0.0);
+    if (x < n2) {
+        hv = h_entry(d, G, sm_h, int(x / n), int(x % n), st);
+        d.h[x] = hv;
+    }
+    if (d.ozb) h_digits(d, hv, int(x));
+}
+
+__device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx);
+
 __device__ __forceinline__ void prep_body(const Dev &d, int k, int bx)
+{
+    const int pair_blocks = prep_pair_blocks(d.n2);
+    if (bx >= pair_blocks) prep_h_part(d, k, bx - pair_blocks);
+    else prep_pair_part(d, k, bx);
+}
+
+// the Psi, Pi and collision tables: one (alpha, beta) pair per warp
+__device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx)
 {
     if (!*d.active) return;
     const StageP st = d.cur->st[k];
     const int n = d.n, Ns = d.Ns, Nb = d.Nb, nv = d.nv;
     const long long n2 = (long long)n * n;
     const double2 *__restrict__ G = g1_stage(d, k);
-    const int pair_blocks = prep_pair_blocks(n2);
-    if (bx >= pair_blocks) {
-        extern __shared__ double2 sm_h[];
-        for (int p = threadIdx.x; p < n; p += blockDim.x) sm_h[p] = G[(long long)p * n + p];
-        __syncthreads();
-        const long long x = (long long)(bx - pair_blocks) * blockDim.x + threadIdx.x;
-        double2 hv = make_double2(0.0, 0.0);
-        if (x < n2) {
-            hv = h_entry(d, G, sm_h, int(x / n), int(x % n), st);
-            d.h[x] = hv;
-        }
-        if (d.ozb) h_digits(d, hv, int(x));
-        return;
-    }
     extern __shared__ double2 sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double2 *wE = sm + warp * (4 * kMaxN);   // n entries
@@ -661,13 +678,18 @@ struct ApplyTcCfg {
 
 inline bool apply_tc_ok(int n) { return n >= 16 && n <= 48; }
 
+// doubles per plane: NP x LDD plus 2, so that the planes of consecutive
+// matrices start 4 banks apart (the rows half stages NB matrices with the
+// matrix index fastest)
+__host__ __device__ inline int apply_tc_plane(int NP, int LDD) { return NP * LDD + 2; }
+
 inline ApplyTcCfg make_apply_tc_cfg(int n, size_t *smem_ab, size_t *smem_cd)
 {
     ApplyTcCfg c;
     c.NP = (n + 15) / 16 * 16;
     c.LDD = c.NP + 12;
     const int tpm = (c.NP / 16) * (c.NP / 16);
-    const size_t plane = size_t(c.NP) * c.LDD * sizeof(double);
+    const size_t plane = size_t(apply_tc_plane(c.NP, c.LDD)) * sizeof(double);
     c.NB = std::max(1, std::min(n * n, 16 / tpm));
     while (c.NB > 1 && (4 + 2 * size_t(c.NB)) * plane + size_t(n) * n * sizeof(double2) > 200 * 1024) c.NB--;
     c.threads = c.NB * tpm * 32;
@@ -691,7 +713,7 @@ __device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTc
     const long long n2 = d.n2, n4 = d.n4;
     const long long m0 = (long long)bx * NB;
     const int nm = int(min((long long)NB, n2 - m0));
-    const int PL = NP * LDD;
+    const int PL = apply_tc_plane(NP, LDD);
     extern __shared__ double smtc[];
     double *Lr = smtc, *Li = Lr + PL, *Rr = Li + PL, *Ri = Rr + PL;
     double *Xp = Ri + PL;  // NB x (real, imaginary) planes
@@ -778,8 +800,10 @@ __device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTc
                     dmma_f64(yi[i][j][0], yi[i][j][1], ai[i], br[j]);
                 }
         };
-        for (int k0 = 0; k0 < NP; k0 += 4) step(Lr, Li, Xr, Xi, k0);  // L X
-        for (int k0 = 0; k0 < NP; k0 += 4) step(Xr, Xi, Rr, Ri, k0);  // X R
+        // the contraction index runs over n rounded up to 4 (the rest is padding)
+        const int KN = (n + 3) & ~3;
+        for (int k0 = 0; k0 < KN; k0 += 4) step(Lr, Li, Xr, Xi, k0);  // L X
+        for (int k0 = 0; k0 < KN; k0 += 4) step(Xr, Xi, Rr, Ri, k0);  // X R
     }
     __syncthreads();  // every warp has read the X planes
     if (live) {
