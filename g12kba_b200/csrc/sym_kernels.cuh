@@ -204,8 +204,8 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
     const double2 *__restrict__ Qo = d.Q + t * n3;
     const double2 *__restrict__ Qt = s.Qt + t * n3;
     const double2 *__restrict__ Rtt = s.Rtt;
-    double2 *__restrict__ Yc = s.Yc + ((long long)t * s.npairs + p) * kTB * kTB;
-    double2 *__restrict__ Ac = s.Ac + ((long long)t * s.npairs + p) * kTB * kTB;
+    double2 *Yc = s.Yc + ((long long)t * s.npairs + p) * kTB * kTB;
+    double2 *Ac = s.Ac + ((long long)t * s.npairs + p) * kTB * kTB;
     auto vdist = [&](int s1, int s2) -> double {
         const int m = abs(s1 - s2);
         return (m >= 1 && m <= d.nv) ? U * d.law[m - 1] : 0.0;
@@ -248,23 +248,14 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
         __syncthreads();
         const double2 g22 = Gs[mu2 * GLD + nu2];
         fused = !diag && !d.debug;
-        double2 *__restrict__ Dt = d.D + t * n3;
-        const double2 *__restrict__ RttJ = Rtt + (long long)sj * n * n;
-        const double2 *__restrict__ RttL = Rtt + (long long)sl * n * n;
-        const double2 *__restrict__ QtM = Qt + (long long)mu2 * n * n;
-        const double2 *__restrict__ QtN = Qt + (long long)nu2 * n * n;
+        double2 *Dt = d.D + t * n3;
+        const double2 *RttJ = Rtt + (long long)sj * n * n, *RttL = Rtt + (long long)sl * n * n;
+        const double2 *QtM = Qt + (long long)mu2 * n * n, *QtN = Qt + (long long)nu2 * n * n;
 #pragma unroll 4
         for (int j = 0; j < kTB * kTB / 256; ++j) {
             const int cl = (threadIdx.x >> 5) + 8 * j;
             const int e = cl * kTB + rl;  // = threadIdx.x + 256 j
             const int nu1 = c0 + cl;
-            // every global read of this element first, so that they are in
-            // flight together (one round trip to L2 per element, not three)
-            const double2 rJ = RttJ[nu1 * n + mu1], rL = RttL[nu1 * n + mu1];
-            const double2 qM = QtM[nu1 * n + mu1], qN = QtN[nu1 * n + mu1];
-            const bool rk_here = fused;
-            const double2 yv = rk_here ? Yc[e] : make_double2(0.0, 0.0);
-            const double2 av = (rk_here && k > 0) ? Ac[e] : make_double2(0.0, 0.0);
             const T2 w1 = Wrc[cl * (kTB + 1) + rl];
             const T2 w2 = Wcr[rl * (kTB + 1) + cl];
             const double2 C = make_double2(double(w1.x) - double(w2.x), double(w1.y) + double(w2.y));
@@ -272,7 +263,7 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
             const double2 g1122 = c_mul(g11, g22);
             const double wd = wa - wb[cl];
             double2 psi = c_scale(g1122, wd);
-            psi = c_add(psi, c_i(c_mul(g22, c_sub(rJ, rL))));
+            psi = c_add(psi, c_i(c_mul(g22, c_sub(RttJ[nu1 * n + mu1], RttL[nu1 * n + mu1]))));
             psi = c_add(psi, c_i(c_mul(g11, c_sub(ra, rb[cl]))));
             if (t == 0) {
                 psi = c_sub(psi, c_scale(g1122, U * (double(mu1 == mu2) - double(nu1 == nu2))));
@@ -280,18 +271,18 @@ __global__ void __launch_bounds__(256, 4) k_sym_epi(SymDev s, int k)
                 const double2 e2 = c_sub(fa, hb[cl]);
                 psi = c_add(psi, c_scale(c_mi(c_add(c_mul(g22, e1), c_mul(g11, e2))), U));
             }
-            const double2 pi = c_mul(g22, c_sub(qM, qN));
+            const double2 pi = c_mul(g22, c_sub(QtM[nu1 * n + mu1], QtN[nu1 * n + mu1]));
             const double2 piP = c_mul(Gs[nu1 * GLD + mu1], c_sub(qb[cl], qa));
             const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
-            if (rk_here) {
+            if (fused) {
                 // RK4 bookkeeping of this element right away (off-diagonal tile pairs)
-                const double2 rk = c_add(av, c_scale(K, st.w));
+                const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : Ac[e], c_scale(K, st.w));
                 double2 v;
                 if (k < 3) {
                     Ac[e] = rk;
-                    v = c_add(yv, c_scale(K, st.c_next));
+                    v = c_add(Yc[e], c_scale(K, st.c_next));
                 } else {
-                    v = c_add(yv, c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
+                    v = c_add(Yc[e], c_scale(c_scale(rk, st.dt), 1.0 / 6.0));
                     Yc[e] = v;
                 }
                 Ks[cl * KLD + rl] = v;
