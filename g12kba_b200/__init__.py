@@ -147,6 +147,8 @@ def lib():
         L.g12_mlp_train_pushforward.argtypes = [_vp, _vp, C.c_int32, C.c_int64, _i64p, C.c_int32, C.c_int32,
                                                 C.c_float, C.c_float, C.c_float, _dp]
         L.g12_mlp_rollout.argtypes = [_vp, _vp, C.c_int32, C.c_int64, C.c_int64, _fp]
+        L.g12_mlp_judge.argtypes = [_vp, _vp, _vp, C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.c_double,
+                                    C.POINTER(C.c_int64)]
         _lib = L
     return _lib
 

@@ -842,6 +842,95 @@ extern "C" int g12_mlp_rollout(g12_mlp *m, float *feat_dev, int32_t ntraj, int64
     return check_err(m);
 }
 
+namespace {
+
+// dipole.h:25-32 of one snapshot's features (Im G1_ii = Re rho_ii sits at the
+// upper-triangle index i n - i (i - 1) / 2 of the real parts)
+__device__ __forceinline__ double feat_dipole(const float *f, int n)
+{
+    double p = 0.0;
+    for (int i = 0; i < n / 2; ++i) {
+        const int a = i * n - i * (i - 1) / 2, j = n - 1 - i, b2 = j * n - j * (j - 1) / 2;
+        p += 2.0 * (n / 2.0 - i - 0.5) * (double(f[a]) - double(f[b2])) / n;
+    }
+    return p;
+}
+
+// One block per trajectory: max |p_ref| after t0, then the maximum of
+// |p_pred - p_ref| / max |p_ref| over each checkpoint interval (atomicMax on
+// the bits of nonnegative doubles), then the first failing checkpoint.
+__global__ void __launch_bounds__(256) k_judge(const float *pred, const float *ref, long long snaps, long long t0, int n,
+                                               int every, int nck, double tol, long long *accepted)
+{
+    extern __shared__ unsigned long long ivmax[];  // nck interval maxima
+    __shared__ double red[256];
+    const int F = n * (n + 1);
+    const float *P = pred + (long long)blockIdx.x * snaps * F;
+    const float *Rf = ref + (long long)blockIdx.x * snaps * F;
+    const long long T = snaps - 1 - t0;
+    double amp = 0.0;
+    for (long long s = threadIdx.x; s < T; s += blockDim.x) amp = fmax(amp, fabs(feat_dipole(Rf + (t0 + 1 + s) * F, n)));
+    red[threadIdx.x] = amp;
+    for (int x = threadIdx.x; x < nck; x += blockDim.x) ivmax[x] = 0ull;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    amp = fmax(red[0], 1e-12);
+    for (long long s = threadIdx.x; s < (long long)nck * every; s += blockDim.x) {
+        const long long q = (t0 + 1 + s) * F;
+        const double e = fabs(feat_dipole(P + q, n) - feat_dipole(Rf + q, n)) / amp;
+        atomicMax(&ivmax[s / every], (unsigned long long)__double_as_longlong(e));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long acc = T;
+        double run = 0.0;
+        for (int j = 0; j < nck; ++j) {
+            run = fmax(run, __longlong_as_double((long long)ivmax[j]));
+            if (run > tol) {
+                acc = (long long)j * every;
+                break;
+            }
+        }
+        accepted[blockIdx.x] = acc;
+    }
+}
+
+}  // namespace
+
+extern "C" int g12_mlp_judge(g12_mlp *m, const float *pred_dev, const float *ref_dev, int32_t ntraj, int64_t snaps,
+                             int64_t t0, int32_t every, double tol, int64_t *accepted_out)
+{
+    if (!m || !m->has_norm || !pred_dev || !ref_dev || !accepted_out || ntraj < 1 || every < 1 || t0 < 0 ||
+        t0 >= snaps - 1)
+        return G12_ERR_INVALID;
+    const int F = m->norm.F;
+    int n = 0;
+    while ((n + 1) * (n + 2) <= F) ++n;
+    if (n * (n + 1) != F) return G12_ERR_INVALID;
+    const long long nck = (snaps - 1 - t0) / every;  // full checkpoint intervals
+    if (nck > 6000) {
+        m->err = "g12_mlp_judge: more than 6000 checkpoints";
+        return G12_ERR_INVALID;
+    }
+    MCK(cudaSetDevice(m->device));
+    long long *acc_d = nullptr;
+    MCK(cudaMallocAsync(&acc_d, sizeof(long long) * ntraj, m->s));
+    k_judge<<<ntraj, 256, sizeof(unsigned long long) * std::max<long long>(nck, 1), m->s>>>(
+        pred_dev, ref_dev, snaps, t0, n, every, int(nck), tol, acc_d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(accepted_out, acc_d, sizeof(long long) * ntraj, cudaMemcpyDeviceToHost, m->s);
+    cudaFreeAsync(acc_d, m->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->s);
+    if (e != cudaSuccess) {
+        m->err = std::string("g12_mlp_judge: ") + cudaGetErrorString(e);
+        return G12_ERR_CUDA;
+    }
+    return G12_OK;
+}
+
 // One optimisation step after `r` blocks of the network's own rollout
 // ("pushforward" training): windows start at (traj, t) of feat_dev, the network
 // predicts r blocks of M snapshots from them (no gradient through those), and

@@ -426,18 +426,19 @@ def judged_rollout(ex, params, prefix_states, prefix_feat, total, check_every=20
         f, _, ms = _rk4_features(params[i], prefix_states[i], T - P, precision, device)
         rk_feat[int(i)] = f
         rk_ms += ms
-    # running dipole error of the judged trajectories at the checkpoints
-    accepted = T - P
-    for c in range(check_every, T - P + 1, check_every):
-        worst = 0.0
-        for i in judged:
-            pr = dipole_from_features(out[i, P:P + c], n)
-            pt = dipole_from_features(rk_feat[int(i)][:c], n)
-            full = dipole_from_features(rk_feat[int(i)], n)
-            worst = max(worst, float(np.max(np.abs(pr - pt)) / max(np.max(np.abs(full)), 1e-12)))
-        if worst > tol:
-            accepted = c - check_every
-            break
+    # the judge on the device (g12_mlp_judge): running dipole error of every
+    # judged trajectory at the checkpoints; accepted up to the last checkpoint
+    # that all of them pass
+    ref = pred[torch.as_tensor(judged, device=pred.device)].clone()
+    for r, i in enumerate(judged):
+        ref[r, P:] = torch.from_numpy(rk_feat[int(i)]).to(pred.device)
+    sel = pred[torch.as_tensor(judged, device=pred.device)].contiguous()
+    acc = np.zeros(len(judged), np.int64)
+    torch.cuda.synchronize()
+    ex.mlp._chk(lib().g12_mlp_judge(ex.mlp.h, C.c_void_p(sel.data_ptr()), C.c_void_p(ref.data_ptr()), len(judged),
+                                    T, P - 1, check_every, tol, acc.ctypes.data_as(C.POINTER(C.c_int64))))
+    # snapshots accepted after the prefix (the judge counts from snapshot P)
+    accepted = int(acc.min())
     fallback = accepted < T - P
     fb_ms = 0.0
     if fallback:

@@ -276,6 +276,15 @@ int g12_mlp_train_pushforward(g12_mlp *m, const float *feat_dev, int32_t ntraj, 
 /* in place: snapshots t0+1 .. snaps-1 of every trajectory from blocks of M
  * predictions ((snaps-1-t0) % M == 0); device time in *elapsed_ms */
 int g12_mlp_rollout(g12_mlp *m, float *feat_dev, int32_t ntraj, int64_t snaps, int64_t t0, float *elapsed_ms);
+/* The plain-RK4 judge of a rollout: pred_dev and ref_dev [ntraj][snaps][F]
+ * (the network's and the RK4 snapshot features of the same trajectories, F as
+ * set by g12_mlp_set_norm); the dipole (dipole.h:25-32) of both after t0, the
+ * running maximum of |p_pred - p_ref| / max |p_ref| (the RK4 maximum after
+ * t0), and accepted_out[b] (host) = the snapshots after t0 up to the last
+ * checkpoint (every `every` snapshots) at which it is still <= tol (all
+ * snapshots after t0 when every full checkpoint passes). */
+int g12_mlp_judge(g12_mlp *m, const float *pred_dev, const float *ref_dev, int32_t ntraj, int64_t snaps, int64_t t0,
+                  int32_t every, double tol, int64_t *accepted_out);
 
 /* Batched propagation recording snapshot features (the layout above) of every
  * system after every `every`-th step into feat_dev [nsys][nsteps/every][F]
