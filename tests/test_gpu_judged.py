@@ -48,3 +48,40 @@ def test_accepted_network_output_is_kept(g12):
     pred = pred.cpu().numpy()
     assert np.array_equal(out[:, :P], prefix.cpu().numpy())
     assert np.max(np.abs(out - pred)) <= 1e-3 * np.max(np.abs(pred))
+
+
+def test_device_judge_matches_host_computation(g12):
+    """g12_mlp_judge against the same running dipole error computed on the
+    host (learned.dipole_from_features), on synthetic features."""
+    torch = pytest.importorskip("torch")
+    import ctypes as C
+    from g12kba_b200 import learned as L
+    n, T, P, every = 16, 150, 20, 16
+    F = n * (n + 1)
+    rng = np.random.default_rng(2)
+    ref = rng.standard_normal((4, T, F)).astype(np.float32)
+    pred = ref.copy()
+    # trajectory b drifts from snapshot P + 10 * (b + 1) on, by an amount that
+    # crosses the tolerance a few steps later
+    for b in range(4):
+        s0 = P + 10 * (b + 1)
+        pred[b, s0:] += np.float32(0.02) * np.arange(T - s0, dtype=np.float32)[:, None]
+    ex = L.Extrapolator(n, K=16, M=16, width=128, max_batch=128, seed=1)
+    ex.fit_norm(torch.from_numpy(ref).cuda())
+    tol = 1e-2
+    acc = np.zeros(4, np.int64)
+    pd, rd = torch.from_numpy(pred).cuda(), torch.from_numpy(ref).cuda()
+    torch.cuda.synchronize()
+    ex.mlp._chk(g12.lib().g12_mlp_judge(ex.mlp.h, C.c_void_p(pd.data_ptr()), C.c_void_p(rd.data_ptr()), 4, T, P - 1,
+                                         every, tol, acc.ctypes.data_as(C.POINTER(C.c_int64))))
+    for b in range(4):
+        pp = L.dipole_from_features(pred[b, P:], n)
+        pr = L.dipole_from_features(ref[b, P:], n)
+        err = np.maximum.accumulate(np.abs(pp - pr) / max(np.max(np.abs(pr)), 1e-12))
+        want = T - P
+        for c in range(every, T - P + 1, every):
+            if err[c - 1] > tol:
+                want = c - every
+                break
+        assert acc[b] == want, (b, acc[b], want)
+    assert len(set(acc.tolist())) > 1  # the drifts start at different checkpoints
