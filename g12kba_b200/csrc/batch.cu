@@ -321,7 +321,7 @@ ApplyTcCfg tc_cfg_nb(int n, int nb, size_t *sab, size_t *scd)
     c.NB = nb;
     c.threads = kTcThreads;
     *sab = (4 + 2 * size_t(nb)) * plane;
-    *scd = *sab + size_t(n) * n * sizeof(double2);
+    *scd = *sab + size_t(n) * (n + 1) * sizeof(double2);
     return c;
 }
 

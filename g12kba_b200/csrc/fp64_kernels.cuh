@@ -473,7 +473,7 @@ struct ApplyCfg {
 // Fused epilogue of one element G2[r; nu1 nu2] (r = mu1 + n mu2) of the
 // column half: C = TAB - Y (Y = (M H2) at that element), Psi, Pi, K2
 // (G1_G2_t_step.h:55-86) and the RK4 bookkeeping (RK_solver.h:137-139,
-// 209-213).  Gs: the stage's G1, n x n row-major (shared memory).
+// 209-213).  Gs: the stage's G1, n x n row-major, rows gld apart (shared memory).
 struct ApplyEpi {
     long long r;
     StageP st;
@@ -494,8 +494,9 @@ struct ApplyEpi {
         const int m = abs(s1 - s2);
         return (m >= 1 && m <= d.nv) ? U * d.law[m - 1] : 0.0;
     }
+    // Gs rows are gld apart (n, or n + 1 where consecutive threads read columns)
     __device__ __forceinline__ void element(const Dev &d, int k, int t, int nu1, int nu2, double2 y,
-                                            const double2 *Gs) const
+                                            const double2 *Gs, int gld) const
     {
         const int n = d.n, Ns = d.Ns;
         const long long n2 = d.n2, n4 = d.n4;
@@ -505,22 +506,22 @@ struct ApplyEpi {
         const double2 *Qt = d.Q + t * d.n3;
         const long long x = r * n2 + nu1 + (long long)n * nu2;
         const double2 C = c_sub(d.TAB[t * n4 + x], y);
-        const double2 g11 = Gs[mu1 * n + nu1], g22 = Gs[mu2 * n + nu2];
+        const double2 g11 = Gs[mu1 * gld + nu1], g22 = Gs[mu2 * gld + nu2];
         const double wd = wij - (U * double(sk == sl) + vdist(d, sk, sl));
         double2 psi = c_scale(c_mul(g11, g22), wd);
         psi = c_add(psi, c_i(c_mul(g22, c_sub(Rt1[nu1 * Ns + sj], Rt1[nu1 * Ns + sl]))));
         psi = c_add(psi, c_i(c_mul(g11, c_sub(Rt2[nu2 * Ns + si], Rt2[nu2 * Ns + sk]))));
         if (t == 0) {
             psi = c_sub(psi, c_scale(c_mul(g11, g22), U * (double(mu1 == mu2) - double(nu1 == nu2))));
-            const double2 e1 = c_sub(c_mul(Gs[mu1 * n + mu2], Gs[mu2 * n + nu1]),
-                                     c_mul(Gs[mu1 * n + nu2], Gs[nu2 * n + nu1]));
-            const double2 e2 = c_sub(c_mul(Gs[mu2 * n + mu1], Gs[mu1 * n + nu2]),
-                                     c_mul(Gs[mu2 * n + nu1], Gs[nu1 * n + nu2]));
+            const double2 e1 = c_sub(c_mul(Gs[mu1 * gld + mu2], Gs[mu2 * gld + nu1]),
+                                     c_mul(Gs[mu1 * gld + nu2], Gs[nu2 * gld + nu1]));
+            const double2 e2 = c_sub(c_mul(Gs[mu2 * gld + mu1], Gs[mu1 * gld + nu2]),
+                                     c_mul(Gs[mu2 * gld + nu1], Gs[nu1 * gld + nu2]));
             psi = c_add(psi, c_scale(c_mi(c_add(c_mul(g22, e1), c_mul(g11, e2))), U));
         }
         const long long q1 = ((long long)mu1 * n + nu1) * n, q2 = ((long long)nu2 * n + mu2) * n;
         const double2 pi = c_mul(g22, c_sub(Qt[q1 + mu2], Qt[q1 + nu2]));
-        const double2 piP = c_mul(Gs[nu1 * n + mu1], c_sub(Qt[q2 + nu1], Qt[q2 + mu1]));
+        const double2 piP = c_mul(Gs[nu1 * gld + mu1], c_sub(Qt[q2 + nu1], Qt[q2 + mu1]));
         const double2 K = c_mi(c_sub(c_add(c_add(C, psi), pi), c_conj(piP)));
         if (d.debug) {
             d.TMP0[t * n4 + x] = K;
@@ -651,7 +652,7 @@ __device__ __forceinline__ void apply_body(const Dev &d, int k, const ApplyCfg &
         for (int b = 0; b < 4; ++b) {
             const int nu1 = tj + S * b;
             if (nu1 >= n) continue;
-            ep.element(d, k, t, nu1, nu2, acc[a][b], Gs);
+            ep.element(d, k, t, nu1, nu2, acc[a][b], Gs, n);
         }
     }
 }
@@ -691,10 +692,10 @@ inline ApplyTcCfg make_apply_tc_cfg(int n, size_t *smem_ab, size_t *smem_cd)
     const int tpm = (c.NP / 16) * (c.NP / 16);
     const size_t plane = size_t(apply_tc_plane(c.NP, c.LDD)) * sizeof(double);
     c.NB = std::max(1, std::min(n * n, 8 / tpm));  // 2 matrices per block at n = 32 (6% faster than 4)
-    while (c.NB > 1 && (4 + 2 * size_t(c.NB)) * plane + size_t(n) * n * sizeof(double2) > 200 * 1024) c.NB--;
+    while (c.NB > 1 && (4 + 2 * size_t(c.NB)) * plane + size_t(n) * (n + 1) * sizeof(double2) > 200 * 1024) c.NB--;
     c.threads = c.NB * tpm * 32;
     *smem_ab = (4 + 2 * size_t(c.NB)) * plane;
-    *smem_cd = *smem_ab + size_t(n) * n * sizeof(double2);
+    *smem_cd = *smem_ab + size_t(n) * (n + 1) * sizeof(double2);
     return c;
 }
 
@@ -717,7 +718,7 @@ __device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTc
     extern __shared__ double smtc[];
     double *Lr = smtc, *Li = Lr + PL, *Rr = Li + PL, *Ri = Rr + PL;
     double *Xp = Ri + PL;  // NB x (real, imaginary) planes
-    double2 *Gs = reinterpret_cast<double2 *>(Xp + 2 * NB * PL);  // CD only: n*n
+    double2 *Gs = reinterpret_cast<double2 *>(Xp + 2 * NB * PL);  // CD only: n x (n + 1)
     const double2 *X = g2_stage(d, k) + t * n4;
 
     // (L, R) = (h, h^T) for the rows, (h^T, h) for the columns
@@ -733,8 +734,9 @@ __device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTc
     if (NP != n)
         for (int x = threadIdx.x; x < 2 * NB * PL; x += blockDim.x) Xp[x] = 0.0;
     if (CD) {
+        // rows n + 1 apart: the epilogue's threads read G1 along columns too
         const double2 *G1 = g1_stage(d, k);
-        for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[x] = G1[x];
+        for (int x = threadIdx.x; x < n * n; x += blockDim.x) Gs[(x / n) * (n + 1) + x % n] = G1[x];
     }
     __syncthreads();
     if (!CD) {
@@ -839,7 +841,7 @@ __device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTc
         const int nu1 = c % n, nu2 = c / n;
         const double *P = Xp + 2 * rb * PL;
         const ApplyEpi ep(d, st, m0 + rb);
-        ep.element(d, k, t, nu1, nu2, make_double2(P[nu2 * LDD + nu1], P[PL + nu2 * LDD + nu1]), Gs);
+        ep.element(d, k, t, nu1, nu2, make_double2(P[nu2 * LDD + nu1], P[PL + nu2 * LDD + nu1]), Gs, n + 1);
     }
 }
 
