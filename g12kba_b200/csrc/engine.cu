@@ -489,8 +489,12 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     if (precision != G12_PREC_FP64) {
         int rc = mixed_init(ctx->mixed, d, precision, &ctx->err);
         if (rc) return fail(rc);
-        d.Qt = ctx->mixed.s.Qt;  // k_prep writes the transposed tables the epilogue reads
-        d.Rtt = ctx->mixed.s.Rtt;
+        if (ctx->mixed.epip) {
+            d.Zt = ctx->mixed.Zt;  // k_prep writes the combined table the persistent epilogue reads
+        } else {
+            d.Qt = ctx->mixed.s.Qt;  // k_prep writes the transposed tables the epilogue reads
+            d.Rtt = ctx->mixed.s.Rtt;
+        }
         d.ozb = ctx->mixed.ozb;  // k_prep also writes the digits of h for the tcgen05 GEMM
     }
     if (ensure_sched(ctx, 1024)) return fail(G12_ERR_CUDA);
@@ -661,6 +665,12 @@ extern "C" int g12_rhs(g12_ctx *ctx, const double *G1, const double *G2xx, const
     }
     Dev dd = ctx->d;
     dd.debug = 1;
+    if (ctx->prec != G12_PREC_FP64) {
+        // the per-pair epilogue (the one with the K output) reads the transposed tables
+        dd.Qt = ctx->mixed.s.Qt;
+        dd.Rtt = ctx->mixed.s.Rtt;
+        dd.Zt = nullptr;
+    }
     const int one = 1;
     CK(cudaMemcpyAsync(dd.cur, &sp, sizeof(StepP), cudaMemcpyHostToDevice, ctx->s));
     CK(cudaMemcpyAsync(dd.active, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->s));

@@ -51,6 +51,7 @@ struct Dev {
     double2 *Y1, *G1t0, *G1t1, *RK1, *h, *Ix, *comm_dbg, *K1_dbg;
     double2 *Y2, *RK2, *TMP0, *TMP1, *TAB, *D, *Q, *Rt;
     double2 *Qt, *Rtt;  // transposed table copies (symmetric engine), or null
+    double2 *Zt;        // combined table i Rtt[site(r)] + Qt[t][r] (persistent epilogue at n = 32), or null
     unsigned char *ozb; // bf16 digit tiles of h for the tcgen05 digit GEMM (symmetric engine), or null
     double2 *traj;
     double *dip;
@@ -201,7 +202,9 @@ __device__ __forceinline__ double2 h_entry(const Dev &d, const double2 *G, const
 // Per (alpha, beta) pair, one warp: Psi factor Rt, Pi factors Q_xx / Q_xy and
 // the collision integral; blocks past the pair blocks build h, one entry per
 // thread.  With d.Qt set (symmetric engine) the transposed copies
-// Qt[t][r][b][a] = Q[t][a][b][r] and Rtt[s][b][a] = Rt[a][b][s] are written too.
+// Qt[t][r][b][a] = Q[t][a][b][r] and Rtt[s][b][a] = Rt[a][b][s] are written too;
+// with d.Zt set, their combination Zt[t][r][b][a] = i Rt[a][b][r % Ns] + Q[t][a][b][r]
+// (the Psi and Pi factors that the epilogue multiplies by the same G1 entry).
 constexpr int kPrepWarps = 4;
 
 __host__ __device__ inline int prep_pair_blocks(long long n2) { return int((n2 + kPrepWarps - 1) / kPrepWarps); }
@@ -350,11 +353,12 @@ __device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx)
     }
     __syncwarp();
     // Rt[s] = U R[s] + sum_m V_m (R[s+m] + R[s-m]);  Vp[s] = sum_m V_m (S[s+m] + S[s-m])
-    double2 Vpv[2];
+    double2 Vpv[2], Rtv[2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int sidx = lane + 32 * q;
         Vpv[q] = make_double2(0.0, 0.0);
+        Rtv[q] = Vpv[q];
         if (sidx >= Ns) continue;
         double2 acc = c_scale(wR[sidx], U), vp = make_double2(0.0, 0.0);
         for (int m = 1; m <= nv; ++m) {
@@ -374,6 +378,7 @@ __device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx)
         d.Rt[pair * Ns + sidx] = acc;
         if (d.Rtt) d.Rtt[((long long)sidx * n + beta) * n + alpha] = acc;
         Vpv[q] = vp;
+        Rtv[q] = acc;
     }
     __syncwarp();
 #pragma unroll
@@ -386,6 +391,17 @@ __device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx)
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const int r = lane + 32 * q;
+        double2 rt = make_double2(0.0, 0.0);
+        if (d.Zt) {
+            // Rt[pair][r % Ns], held by lane (r % Ns) % 32 in Rtv[(r % Ns) / 32]
+            const int src = r < n ? r % Ns : 0;
+            double2 a0, a1;
+            a0.x = __shfl_sync(0xffffffffu, Rtv[0].x, src & 31);
+            a0.y = __shfl_sync(0xffffffffu, Rtv[0].y, src & 31);
+            a1.x = __shfl_sync(0xffffffffu, Rtv[1].x, src & 31);
+            a1.y = __shfl_sync(0xffffffffu, Rtv[1].y, src & 31);
+            rt = (src >> 5) ? a1 : a0;
+        }
         if (r >= n) continue;
         const int sidx = r % Ns;
         const double2 S = wS[sidx], vp = wE[kMaxN - 1 - sidx];
@@ -396,6 +412,10 @@ __device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx)
         if (d.Qt) {
             d.Qt[((long long)r * n + beta) * n + alpha] = qx;
             d.Qt[d.n3 + ((long long)r * n + beta) * n + alpha] = qy;
+        }
+        if (d.Zt) {
+            d.Zt[((long long)r * n + beta) * n + alpha] = c_add(c_i(rt), qx);
+            d.Zt[d.n3 + ((long long)r * n + beta) * n + alpha] = c_add(c_i(rt), qy);
         }
         if (r == alpha) d.Ix[pair] = qx;
     }

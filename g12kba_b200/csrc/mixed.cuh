@@ -16,6 +16,7 @@
 #include "sym_kernels.cuh"
 #include "sym_tc.cuh"
 #include "sym_oz.cuh"
+#include "sym_epi_p.cuh"
 
 namespace g12 {
 
@@ -30,6 +31,9 @@ struct MixedState {
     CUtensorMap map_a{}, map_b{};  // TMA views of TMPa / TMPb
     unsigned char *ozb = nullptr;  // h digit tiles (written by k_prep, read by k_sym_gemm_oz2)
     int oz2 = 0;  // bf16 digit GEMM (k_sym_gemm_oz2)
+    bool epip = false;       // persistent epilogue k_sym_epi_p (digit GEMM at n = 32)
+    double2 *Zt = nullptr;   // its combined Psi/Pi table (written by k_prep)
+    int sms = 148;
     size_t epi_smem = 0, simt_smem = 0, tc_smem = 0;
     int tc_grid = 0;
     std::vector<void *> allocs;
@@ -198,6 +202,15 @@ inline int mixed_init(MixedState &m, const Dev &d, int prec, std::string *err)
             return -3;
         }
         m.tc_grid = m.oz2 ? std::min(2 * s.gemm_tiles, sms) : std::min(2 * s.gemm_tiles, 2 * sms);  // oz2: persistent
+        m.sms = sms;
+        if (m.oz2 && n == 32) {
+            if (!mixed_alloc(m, &m.Zt, size_t(2 * n3))) {
+                if (err) *err = "out of device memory (mixed engine)";
+                return -3;
+            }
+            cudaFuncSetAttribute(k_sym_epi_p, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEpiPSmem));
+            m.epip = true;
+        }
     }
     if (cudaGetLastError() != cudaSuccess) {
         if (err) *err = "mixed engine set-up failed";
@@ -286,6 +299,16 @@ inline void mixed_enqueue_kind(MixedState &m, const Dev &d, int k, int, int q, c
         }
     } else {
         const dim3 g(s.npairs, 2);
+        if (m.oz2 && m.tc && m.epip && !d.debug && d.Zt) {
+            // persistent epilogue: one CTA per SM (pair CTAs, then the G1-side CTAs)
+            SymDev sf = s;
+            sf.g1x = fuse_g1 ? int((s.d.n2 + kEpiPThreads - 1) / kEpiPThreads) : 0;
+            const int units = 2 * s.npairs;
+            int G = std::max(m.sms - sf.g1x, (units + kEpiPMaxUnits - 1) / kEpiPMaxUnits);
+            G = std::min(G, units);
+            launch_pdl(k_sym_epi_p, dim3(G + sf.g1x), dim3(kEpiPThreads), kEpiPSmem, st, sf, k);
+            return;
+        }
         if (m.oz2 && m.tc) {
             SymDev sf = s;
             sf.g1x = fuse_g1 ? int((s.d.n2 + 255) / 256) : 0;
