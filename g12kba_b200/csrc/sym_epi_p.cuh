@@ -3,15 +3,21 @@
 // W^H on a tile pair, Psi, Pi, K2, RK4 bookkeeping, next-stage input), organised
 // for the B200 memory system instead of one short-lived block per tile pair:
 //   * one 512-thread CTA per SM walks its tile pairs (u = blockIdx.x + i G);
-//   * the next pair's inputs - both W tiles (FP32), the FP64 state tile and RK4
-//     sum, the two 16 KB slices of the combined Psi/Pi table Zt and the pair's Rt
-//     and Q rows - are copied into a second shared-memory buffer with cp.async
-//     while the current pair is computed (double buffering, 81 KB per buffer);
+//   * the next pair's inputs are copied into a second shared-memory buffer while
+//     the current pair is computed (double buffering, 81 KB per buffer): one
+//     thread issues 1-D bulk copies of the FP64 state tile and RK4 sum, the two
+//     16 KB slices of the combined Psi/Pi table Zt and the pair's Rt and Q rows
+//     (completion on an mbarrier per buffer); every thread copies one 16-byte
+//     chunk of each W tile with cp.async into a bank-swizzled layout;
 //   * G1 is staged once per CTA, not once per tile pair;
 //   * the table terms i g22 (Rtt[site mu2] - Rtt[site nu2]) + g22 (Qt[mu2] -
 //     Qt[nu2]) of the per-pair kernel are read as g22 (Zt[mu2] - Zt[nu2]), two
-//     shared-memory reads instead of four L2 reads per element.
+//     shared-memory reads instead of four L2 reads per element;
+//   * the next-stage input is rounded to FP32 once, into a padded staging tile
+//     that both output tiles (R, C) and (C, R) are written from.
 // CTAs past the pair CTAs (s.g1x of them) run the stage's G1 side (g1_body).
+// Every mbarrier wait is bounded; on expiry the kernel records code 91 in the
+// error word, lets its copies in flight land (bounded) and returns.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -35,7 +41,7 @@ struct EpiPBuf {
     double2 Rt[kTB];                       // Rt[(mu2, nu2)][s], s < Ns
     double2 Qr[kTB];                       // Q[t][nu2][mu2][x], x < n
 };
-constexpr size_t kEpiPSmem = 2 * sizeof(double2) * 32 * 33 + 2 * sizeof(EpiPBuf);
+constexpr size_t kEpiPSmem = 2 * sizeof(double2) * 32 * 33 + 2 * sizeof(EpiPBuf) + sizeof(float2) * 32 * 33;
 
 // float index of element (row rho, column c) of a swizzled W tile
 __device__ __forceinline__ int epip_wsw(int rho, int c) { return rho * kTB + ((((c >> 2) ^ (rho >> 1)) & 7) << 2) + (c & 3); }
@@ -44,6 +50,13 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait()
@@ -51,17 +64,22 @@ __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// copies of tile pair u's FP64 state tiles (written by the previous stage's
-// epilogue: independent of this stage's k_prep and GEMM); 16 bytes per thread and tile
-__device__ __forceinline__ void epip_issue_state(const SymDev &s, int k, EpiPBuf &b, int u)
+// one thread: bulk copies of tile pair u's state tiles, table slices and rows, completing on bar
+__device__ __forceinline__ void epip_issue_bulk(const SymDev &s, int k, int u, int Rb, int Cb, EpiPBuf &b, uint64_t *bar)
 {
-    const double2 *Y = s.Yc + (long long)u * (kTB * kTB), *A = s.Ac + (long long)u * (kTB * kTB);
-    const int x = threadIdx.x;
-#pragma unroll
-    for (int q = 0; q < kTB * kTB / kEpiPThreads; ++q) {
-        cp_async16(&b.Yc[x + q * kEpiPThreads], Y + x + q * kEpiPThreads);
-        if (k > 0) cp_async16(&b.Ac[x + q * kEpiPThreads], A + x + q * kEpiPThreads);
+    constexpr int n = 32, n2 = n * n, n3 = n2 * n;
+    const int t = u / s.npairs;
+    const bool diag = Rb == Cb;
+    const uint32_t tile = kTB * kTB * sizeof(double2);
+    mbar_expect_tx(bar, tile * (1 + (k > 0) + 2 * !diag) + s.d.Ns * sizeof(double2) + n * sizeof(double2));
+    bulk_load(b.Yc, s.Yc + (long long)u * (kTB * kTB), tile, bar);
+    if (k > 0) bulk_load(b.Ac, s.Ac + (long long)u * (kTB * kTB), tile, bar);
+    if (!diag) {
+        bulk_load(b.Zm, s.d.Zt + t * n3 + Rb * n2, tile, bar);
+        bulk_load(b.Zn, s.d.Zt + t * n3 + Cb * n2, tile, bar);
     }
+    bulk_load(b.Rt, s.d.Rt + (Rb * n + Cb) * s.d.Ns, s.d.Ns * sizeof(double2), bar);
+    bulk_load(b.Qr, s.d.Q + t * n3 + (Cb * n + Rb) * n, n * sizeof(double2), bar);
 }
 
 // copies of tile pair (t; mu2 = Rb, nu2 = Cb)'s W tiles, table slices and rows
@@ -69,7 +87,7 @@ __device__ __forceinline__ void epip_issue_state(const SymDev &s, int k, EpiPBuf
 __device__ __forceinline__ void epip_issue_stage(const SymDev &s, int t, int Rb, int Cb, EpiPBuf &b)
 {
     constexpr int n = 32;
-    constexpr int n2 = n * n, n3 = n2 * n;
+    constexpr int n2 = n * n;
     static_assert(2 * kTB * kTB / 4 == kEpiPThreads, "one 16-byte chunk of each W tile per thread");
     const float *Wg = s.W + (long long)t * 2 * s.n4;
     const int R0 = Rb * kTB, C0 = Cb * kTB;
@@ -77,16 +95,6 @@ __device__ __forceinline__ void epip_issue_stage(const SymDev &s, int t, int Rb,
     const int dst = rho * kTB + (((q ^ (rho >> 1)) & 7) << 2);
     cp_async16(&b.Wrc[dst], Wg + (2 * C0 + rho) * n2 + R0 + 4 * q);
     cp_async16(&b.Wcr[dst], Wg + (2 * R0 + rho) * n2 + C0 + 4 * q);
-    if (Rb != Cb) {
-        const double2 *Zm = s.d.Zt + t * n3 + Rb * n2, *Zn = s.d.Zt + t * n3 + Cb * n2;
-#pragma unroll
-        for (int i = 0; i < kTB * kTB / kEpiPThreads; ++i) {
-            cp_async16(&b.Zm[x + i * kEpiPThreads], Zm + x + i * kEpiPThreads);
-            cp_async16(&b.Zn[x + i * kEpiPThreads], Zn + x + i * kEpiPThreads);
-        }
-    }
-    if (x < s.d.Ns) cp_async16(&b.Rt[x], s.d.Rt + (Rb * n + Cb) * s.d.Ns + x);
-    else if (x >= 32 && x < 32 + n) cp_async16(&b.Qr[x - 32], s.d.Q + t * n3 + (Cb * n + Rb) * n + x - 32);
 }
 
 __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
@@ -106,9 +114,11 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     double2 *Gs = reinterpret_cast<double2 *>(smp);  // n x GLD
     double2 *Ks = Gs + n * GLD;                       // [c_l][r_l] K or next input, rows of KLD
     EpiPBuf *buf = reinterpret_cast<EpiPBuf *>(Ks + kTB * KLD);
+    float2 *KF = reinterpret_cast<float2 *>(buf + 2);  // [c_l][r_l] next-stage input (FP32), rows of KLD
     __shared__ int site[n];
     __shared__ double wtab[n];  // pair weight by site distance m: U (m = 0), V_m (m <= nv), 0
     __shared__ int2 urc[kEpiPMaxUnits];
+    __shared__ __align__(8) uint64_t bar[2];
     const int units = 2 * s.npairs;
     const int nu = (units - int(blockIdx.x) + G - 1) / G;
     if (nu <= 0) return;
@@ -127,7 +137,11 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         // the reference's weights U (same site) and V_m (|i - j| = m <= nv): U * double(si == sj) + V
         wtab[m] = m == 0 ? U : (m <= d.nv ? U * d.law[m - 1] : 0.0);
     }
-    epip_issue_state(s, k, buf[0], blockIdx.x);
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     const double2 *G1 = (k & 1) ? d.G1t1 : d.G1t0;
 #pragma unroll
     for (int q = 0; q < n * n / kEpiPThreads; ++q) {
@@ -138,6 +152,7 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     // W comes from the GEMM launched just before this kernel, the tables from
     // k_prep before it (G1 was complete before k_prep started)
     grid_dep_wait();
+    if (threadIdx.x == 0) epip_issue_bulk(s, k, blockIdx.x, urc[0].x, urc[0].y, buf[0], &bar[0]);
     epip_issue_stage(s, int(blockIdx.x) / s.npairs, urc[0].x, urc[0].y, buf[0]);
     cp_async_commit();
 
@@ -148,14 +163,23 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         if (i + 1 < nu) {
             const int u1 = int(blockIdx.x) + (i + 1) * G;
             EpiPBuf &b1 = buf[(i + 1) & 1];
-            epip_issue_state(s, k, b1, u1);
+            if (threadIdx.x == 0) epip_issue_bulk(s, k, u1, urc[i + 1].x, urc[i + 1].y, b1, &bar[(i + 1) & 1]);
             epip_issue_stage(s, u1 / s.npairs, urc[i + 1].x, urc[i + 1].y, b1);
             cp_async_commit();
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
         }
-        __syncthreads();
+        const bool ok = mbar_wait(&bar[i & 1], (i >> 1) & 1);
+        if (!__syncthreads_and(ok)) {
+            // copies did not arrive in time: report, let the ones in flight land, return
+            cp_async_wait<0>();
+            if (threadIdx.x == 0) {
+                atomicExch(s.err, 91);
+                if (i + 1 < nu) mbar_wait(&bar[(i + 1) & 1], ((i + 1) >> 1) & 1);
+            }
+            return;
+        }
         const EpiPBuf &b = buf[i & 1];
         const int u = int(blockIdx.x) + i * G, t = u / s.npairs;
         const int mu2 = urc[i].x, nu2 = urc[i].y;  // n = 32: one mu2 per row block, one nu2 per column block
@@ -229,7 +253,8 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 const int cl = w + 16 * j;
-                Ks[cl * KLD + rl] = rk4(Kv[j], acs[j], ycs[j], cl * kTB + rl);
+                const double2 v = rk4(Kv[j], acs[j], ycs[j], cl * kTB + rl);
+                KF[cl * KLD + rl] = make_float2(float(v.x), float(v.y));
             }
             __syncthreads();
         } else {
@@ -251,7 +276,7 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
             for (int j = 0; j < 2; ++j) {
                 const int cl = w + 16 * j;
                 const double2 v = rk4(sym[j], acs[j], ycs[j], cl * kTB + rl);
-                Ks[cl * KLD + rl] = v;
+                KF[cl * KLD + rl] = make_float2(float(v.x), float(v.y));
                 Dt[(mu1 * n + cl) * n + mu2] = v;
             }
             __syncthreads();
@@ -261,10 +286,10 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const int cl = w + 16 * j;
-            const double2 v = Ks[cl * KLD + rl];
+            const float2 v = KF[cl * KLD + rl];
             const int o = ((mu2 * n * n + nu2 * kTB + cl) * 2) * n + rl;
-            Out[o] = float(v.x);
-            Out[o + n] = float(v.y);
+            Out[o] = v.x;
+            Out[o + n] = v.y;
         }
         if (!diag) {
             // tile (C, R): element (c, r) = conj(v) at tmp_index(n, c_l, nu2, mu2 * 32 + r_l, part),
@@ -272,10 +297,10 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
                 const int rr = w + 16 * j;
-                const double2 v = Ks[rl * KLD + rr];
+                const float2 v = KF[rl * KLD + rr];
                 const int o = ((nu2 * n * n + mu2 * kTB + rr) * 2) * n + rl;
-                Out[o] = float(v.x);
-                Out[o + n] = float(-v.y);
+                Out[o] = v.x;
+                Out[o + n] = -v.y;
             }
         }
     }
