@@ -43,9 +43,6 @@ struct EpiPBuf {
 };
 constexpr size_t kEpiPSmem = 2 * sizeof(double2) * 32 * 33 + 2 * sizeof(EpiPBuf) + sizeof(float2) * 32 * 33;
 
-// float index of element (row rho, column c) of a swizzled W tile
-__device__ __forceinline__ int epip_wsw(int rho, int c) { return rho * kTB + ((((c >> 2) ^ (rho >> 1)) & 7) << 2) + (c & 3); }
-
 __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
@@ -64,37 +61,36 @@ __device__ __forceinline__ void cp_async_wait()
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// one thread: bulk copies of tile pair u's state tiles, table slices and rows, completing on bar
-__device__ __forceinline__ void epip_issue_bulk(const SymDev &s, int k, int u, int Rb, int Cb, EpiPBuf &b, uint64_t *bar)
+// a tile pair of this CTA: row block Rb = mu2, column block Cb = nu2 (n = 32),
+// tensor t, unit index u = t npairs + pair index
+struct EpiPUnit {
+    int Rb, Cb, t, u;
+};
+
+// one thread: bulk copies of a tile pair's state tiles, table slices and rows, completing on bar
+__device__ __forceinline__ void epip_issue_bulk(const SymDev &s, int k, const EpiPUnit &un, EpiPBuf &b, uint64_t *bar)
 {
     constexpr int n = 32, n2 = n * n, n3 = n2 * n;
-    const int t = u / s.npairs;
-    const bool diag = Rb == Cb;
+    const bool diag = un.Rb == un.Cb;
     const uint32_t tile = kTB * kTB * sizeof(double2);
     mbar_expect_tx(bar, tile * (1 + (k > 0) + 2 * !diag) + s.d.Ns * sizeof(double2) + n * sizeof(double2));
-    bulk_load(b.Yc, s.Yc + (long long)u * (kTB * kTB), tile, bar);
-    if (k > 0) bulk_load(b.Ac, s.Ac + (long long)u * (kTB * kTB), tile, bar);
+    bulk_load(b.Yc, s.Yc + (long long)un.u * (kTB * kTB), tile, bar);
+    if (k > 0) bulk_load(b.Ac, s.Ac + (long long)un.u * (kTB * kTB), tile, bar);
     if (!diag) {
-        bulk_load(b.Zm, s.d.Zt + t * n3 + Rb * n2, tile, bar);
-        bulk_load(b.Zn, s.d.Zt + t * n3 + Cb * n2, tile, bar);
+        bulk_load(b.Zm, s.d.Zt + un.t * n3 + un.Rb * n2, tile, bar);
+        bulk_load(b.Zn, s.d.Zt + un.t * n3 + un.Cb * n2, tile, bar);
     }
-    bulk_load(b.Rt, s.d.Rt + (Rb * n + Cb) * s.d.Ns, s.d.Ns * sizeof(double2), bar);
-    bulk_load(b.Qr, s.d.Q + t * n3 + (Cb * n + Rb) * n, n * sizeof(double2), bar);
+    bulk_load(b.Rt, s.d.Rt + (un.Rb * n + un.Cb) * s.d.Ns, s.d.Ns * sizeof(double2), bar);
+    bulk_load(b.Qr, s.d.Q + un.t * n3 + (un.Cb * n + un.Rb) * n, n * sizeof(double2), bar);
 }
 
-// copies of tile pair (t; mu2 = Rb, nu2 = Cb)'s W tiles, table slices and rows
-// (produced by this stage's GEMM and k_prep)
-__device__ __forceinline__ void epip_issue_stage(const SymDev &s, int t, int Rb, int Cb, EpiPBuf &b)
+// every thread: its 16-byte chunk (source offset src, swizzled destination dst)
+// of both W tiles of a tile pair; Wt = W of the pair's tensor
+__device__ __forceinline__ void epip_issue_w(const float *Wt, const EpiPUnit &un, EpiPBuf &b, int dst, int src)
 {
-    constexpr int n = 32;
-    constexpr int n2 = n * n;
-    static_assert(2 * kTB * kTB / 4 == kEpiPThreads, "one 16-byte chunk of each W tile per thread");
-    const float *Wg = s.W + (long long)t * 2 * s.n4;
-    const int R0 = Rb * kTB, C0 = Cb * kTB;
-    const int x = threadIdx.x, rho = x >> 3, q = x & 7;  // 8 threads per 128-byte row
-    const int dst = rho * kTB + (((q ^ (rho >> 1)) & 7) << 2);
-    cp_async16(&b.Wrc[dst], Wg + (2 * C0 + rho) * n2 + R0 + 4 * q);
-    cp_async16(&b.Wcr[dst], Wg + (2 * R0 + rho) * n2 + C0 + 4 * q);
+    constexpr int n2 = 32 * 32;
+    cp_async16(&b.Wrc[dst], Wt + (2 * un.Cb * kTB) * n2 + un.Rb * kTB + src);
+    cp_async16(&b.Wcr[dst], Wt + (2 * un.Rb * kTB) * n2 + un.Cb * kTB + src);
 }
 
 __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
@@ -108,36 +104,40 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         g1_body(d, k, int(blockIdx.x) - G);
         return;
     }
-    constexpr int n = 32, GLD = n + 1, KLD = kTB + 1;
+    constexpr int n = 32, n2 = n * n, GLD = n + 1, KLD = kTB + 1;
     constexpr int n3 = n * n * n;
+    static_assert(2 * kTB * kTB / 4 == kEpiPThreads, "one 16-byte chunk of each W tile per thread");
     extern __shared__ __align__(16) unsigned char smp[];
     double2 *Gs = reinterpret_cast<double2 *>(smp);  // n x GLD
-    double2 *Ks = Gs + n * GLD;                       // [c_l][r_l] K or next input, rows of KLD
+    double2 *Ks = Gs + n * GLD;                       // [c_l][r_l] K of a diagonal pair, rows of KLD
     EpiPBuf *buf = reinterpret_cast<EpiPBuf *>(Ks + kTB * KLD);
     float2 *KF = reinterpret_cast<float2 *>(buf + 2);  // [c_l][r_l] next-stage input (FP32), rows of KLD
     __shared__ int site[n];
     __shared__ double wtab[n];  // pair weight by site distance m: U (m = 0), V_m (m <= nv), 0
-    __shared__ int2 urc[kEpiPMaxUnits];
+    __shared__ EpiPUnit units[kEpiPMaxUnits];
     __shared__ __align__(8) uint64_t bar[2];
-    const int units = 2 * s.npairs;
-    const int nu = (units - int(blockIdx.x) + G - 1) / G;
+    const int tid = threadIdx.x;
+    const int nu = (2 * s.npairs - int(blockIdx.x) + G - 1) / G;
     if (nu <= 0) return;
     if (nu > kEpiPMaxUnits) {
         // grid too small for the unit table (the host sizes it): report, skip the stage
-        if (threadIdx.x == 0) atomicExch(s.err, 90);
+        if (tid == 0) atomicExch(s.err, 90);
         return;
     }
     // step scalars (k_step_begin finished before k_prep started)
     const StageP st = d.cur->st[k];
     const double U = st.U;
-    if (int(threadIdx.x) < nu) urc[threadIdx.x] = s.pairs[(int(blockIdx.x) + int(threadIdx.x) * G) % s.npairs];
-    if (threadIdx.x < n) {
-        const int m = threadIdx.x;
-        site[m] = m % d.Ns;
-        // the reference's weights U (same site) and V_m (|i - j| = m <= nv): U * double(si == sj) + V
-        wtab[m] = m == 0 ? U : (m <= d.nv ? U * d.law[m - 1] : 0.0);
+    if (tid < nu) {
+        const int u = int(blockIdx.x) + tid * G, t = u >= s.npairs ? 1 : 0;
+        const int2 rc = s.pairs[u - t * s.npairs];
+        units[tid] = EpiPUnit{rc.x, rc.y, t, u};
     }
-    if (threadIdx.x == 0) {
+    if (tid < n) {
+        site[tid] = tid % d.Ns;
+        // the reference's weights U (same site) and V_m (|i - j| = m <= nv): U * double(si == sj) + V
+        wtab[tid] = tid == 0 ? U : (tid <= d.nv ? U * d.law[tid - 1] : 0.0);
+    }
+    if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -145,26 +145,49 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     const double2 *G1 = (k & 1) ? d.G1t1 : d.G1t0;
 #pragma unroll
     for (int q = 0; q < n * n / kEpiPThreads; ++q) {
-        const int x = threadIdx.x + q * kEpiPThreads;
+        const int x = tid + q * kEpiPThreads;
         Gs[(x / n) * GLD + x % n] = G1[x];
     }
+    // Per-thread constants.  Copies: chunk cq of W tile row crho, 16-byte chunks
+    // of a row swizzled: element (row rho, column c) at rho * 32 + ((((c >> 2) ^
+    // (rho >> 1)) & 7) << 2) + (c & 3).  Reads: element (r_l, c_l) = (lane, w + 16 j),
+    // e = c_l * 32 + r_l; its W offsets in the direct tile (rho = 2 c_l + part,
+    // c = r_l) and the transposed tile (rho = 2 r_l + part, c = c_l) do not depend
+    // on the pair.
+    const int crho = tid >> 3, cq = tid & 7;
+    const int wdst = crho * kTB + (((cq ^ (crho >> 1)) & 7) << 2), wsrc = crho * n2 + 4 * cq;
+    const int rl = tid & 31, w = tid >> 5;
+    const int ow1 = 2 * w * kTB + ((((rl >> 2) ^ w) & 7) << 2) + (rl & 3);
+    const int ow2[2] = {2 * rl * kTB + ((((w >> 2) ^ rl) & 7) << 2) + (w & 3),
+                        2 * rl * kTB + (((((w >> 2) + 4) ^ rl) & 7) << 2) + (w & 3)};
+    const int e0 = w * kTB + rl;    // element j = 0 (j = 1: + 512)
+    const int og11 = rl * GLD + w;  // Gs[mu1][c_l] (j = 1: + 16); also KF / Ks at row r_l, column c_l
+    const int ogT = w * GLD + rl;   // Gs[c_l][mu1] (j = 1: + 16 GLD); also KF / Ks at row c_l, column r_l
+    const int oo = w * 2 * n + rl;  // output offset inside a tile's rows (j = 1: + 16 * 2n)
+    const float *Wt0 = s.W, *Wt1 = s.W + 2 * s.n4;
+    float *const Out0 = sym_out<float>(s, k), *const Out1 = Out0 + 2 * s.n4;
+    const int mu1 = rl;
     __syncthreads();
+    const int si = site[mu1];
+    int sk[2];
+    sk[0] = site[w];
+    sk[1] = site[w + 16];
     // W comes from the GEMM launched just before this kernel, the tables from
     // k_prep before it (G1 was complete before k_prep started)
     grid_dep_wait();
-    if (threadIdx.x == 0) epip_issue_bulk(s, k, blockIdx.x, urc[0].x, urc[0].y, buf[0], &bar[0]);
-    epip_issue_stage(s, int(blockIdx.x) / s.npairs, urc[0].x, urc[0].y, buf[0]);
-    cp_async_commit();
-
-    const int rl = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int mu1 = rl, si = site[mu1];
-    float *const Out0 = sym_out<float>(s, k);
+    {
+        const EpiPUnit un = units[0];
+        if (tid == 0) epip_issue_bulk(s, k, un, buf[0], &bar[0]);
+        epip_issue_w(un.t ? Wt1 : Wt0, un, buf[0], wdst, wsrc);
+        cp_async_commit();
+    }
     for (int i = 0; i < nu; ++i) {
         if (i + 1 < nu) {
-            const int u1 = int(blockIdx.x) + (i + 1) * G;
+            // buffer (i + 1) & 1 was last read by pair i - 1, before the barrier after its K pass
+            const EpiPUnit un1 = units[i + 1];
             EpiPBuf &b1 = buf[(i + 1) & 1];
-            if (threadIdx.x == 0) epip_issue_bulk(s, k, u1, urc[i + 1].x, urc[i + 1].y, b1, &bar[(i + 1) & 1]);
-            epip_issue_stage(s, u1 / s.npairs, urc[i + 1].x, urc[i + 1].y, b1);
+            if (tid == 0) epip_issue_bulk(s, k, un1, b1, &bar[(i + 1) & 1]);
+            epip_issue_w(un1.t ? Wt1 : Wt0, un1, b1, wdst, wsrc);
             cp_async_commit();
             cp_async_wait<1>();
         } else {
@@ -174,15 +197,16 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         if (!__syncthreads_and(ok)) {
             // copies did not arrive in time: report, let the ones in flight land, return
             cp_async_wait<0>();
-            if (threadIdx.x == 0) {
+            if (tid == 0) {
                 atomicExch(s.err, 91);
                 if (i + 1 < nu) mbar_wait(&bar[(i + 1) & 1], ((i + 1) >> 1) & 1);
             }
             return;
         }
         const EpiPBuf &b = buf[i & 1];
-        const int u = int(blockIdx.x) + i * G, t = u / s.npairs;
-        const int mu2 = urc[i].x, nu2 = urc[i].y;  // n = 32: one mu2 per row block, one nu2 per column block
+        const EpiPUnit un = units[i];
+        const int t = un.t;
+        const int mu2 = un.Rb, nu2 = un.Cb;  // n = 32: one mu2 per row block, one nu2 per column block
         const bool diag = mu2 == nu2;
         const int sj = site[mu2], sl = site[nu2];
         // per-row (mu1 = lane) values of this pair
@@ -202,24 +226,23 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         double2 rb[2], qb[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const int cl = w + 16 * j, e = cl * kTB + rl;
-            const float w1x = b.Wrc[epip_wsw(2 * cl, rl)], w1y = b.Wrc[epip_wsw(2 * cl + 1, rl)];
-            const float w2x = b.Wcr[epip_wsw(2 * rl, cl)], w2y = b.Wcr[epip_wsw(2 * rl + 1, cl)];
+            const int e = e0 + j * 16 * kTB;
+            const float w1x = b.Wrc[ow1 + j * 32 * kTB], w1y = b.Wrc[ow1 + j * 32 * kTB + kTB];
+            const float w2x = b.Wcr[ow2[j]], w2y = b.Wcr[ow2[j] + kTB];
             C[j] = make_double2(double(w1x) - double(w2x), double(w1y) + double(w2y));
-            g11[j] = Gs[mu1 * GLD + cl];
-            gT[j] = Gs[cl * GLD + mu1];
+            g11[j] = Gs[og11 + 16 * j];
+            gT[j] = Gs[ogT + 16 * GLD * j];
             zd[j] = diag ? make_double2(0.0, 0.0) : c_sub(b.Zm[e], b.Zn[e]);
             acs[j] = b.Ac[e];
             ycs[j] = b.Yc[e];
-            const int sk = site[cl];
-            wb[j] = wtab[abs(sk - sl)];
-            rb[j] = b.Rt[sk];
-            qb[j] = b.Qr[cl];
+            wb[j] = wtab[abs(sk[j] - sl)];
+            rb[j] = b.Rt[sk[j]];
+            qb[j] = b.Qr[w + 16 * j];
         }
         double2 Kv[2];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const int cl = w + 16 * j, nu1 = cl;
+            const int nu1 = w + 16 * j;
             const double2 g1122 = c_mul(g11[j], g22);
             double2 psi = c_scale(g1122, wa - wb[j]);
             psi = c_add(psi, c_i(c_mul(g11[j], c_sub(ra, rb[j]))));
@@ -235,7 +258,7 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
             const double2 piP = c_mul(gT[j], c_sub(qb[j], qa));
             Kv[j] = c_mi(c_sub(acc, c_conj(piP)));
         }
-        double2 *Ycg = s.Yc + (long long)u * (kTB * kTB), *Acg = s.Ac + (long long)u * (kTB * kTB);
+        double2 *Ycg = s.Yc + (long long)un.u * (kTB * kTB), *Acg = s.Ac + (long long)un.u * (kTB * kTB);
         // RK4 bookkeeping of one element (RK_solver.h:137-139, 209-213) on the compressed state
         auto rk4 = [&](double2 K, double2 ac, double2 yc, int e) -> double2 {
             const double2 rk = c_add(k == 0 ? make_double2(0.0, 0.0) : ac, c_scale(K, st.w));
@@ -252,55 +275,50 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         if (!diag) {
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int cl = w + 16 * j;
-                const double2 v = rk4(Kv[j], acs[j], ycs[j], cl * kTB + rl);
-                KF[cl * KLD + rl] = make_float2(float(v.x), float(v.y));
+                const double2 v = rk4(Kv[j], acs[j], ycs[j], e0 + j * 16 * kTB);
+                KF[ogT + 16 * KLD * j] = make_float2(float(v.x), float(v.y));
             }
             __syncthreads();
         } else {
             // keep the diagonal block exactly Hermitian: K <- (K + K^H) / 2, then the
             // bookkeeping and the particle-2 diagonal D (mu2 == nu2 on these pairs)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) Ks[(w + 16 * j) * KLD + rl] = Kv[j];
+            for (int j = 0; j < 2; ++j) Ks[ogT + 16 * KLD * j] = Kv[j];
             __syncthreads();
             double2 sym[2];
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int cl = w + 16 * j;
-                const double2 a = Ks[cl * KLD + rl], bb = c_conj(Ks[rl * KLD + cl]);
+                const double2 a = Ks[ogT + 16 * KLD * j], bb = c_conj(Ks[og11 + 16 * j]);
                 sym[j] = make_double2(0.5 * (a.x + bb.x), 0.5 * (a.y + bb.y));
             }
             __syncthreads();
             double2 *Dt = d.D + t * n3;
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int cl = w + 16 * j;
-                const double2 v = rk4(sym[j], acs[j], ycs[j], cl * kTB + rl);
-                KF[cl * KLD + rl] = make_float2(float(v.x), float(v.y));
-                Dt[(mu1 * n + cl) * n + mu2] = v;
+                const double2 v = rk4(sym[j], acs[j], ycs[j], e0 + j * 16 * kTB);
+                KF[ogT + 16 * KLD * j] = make_float2(float(v.x), float(v.y));
+                Dt[(mu1 * n + w + 16 * j) * n + mu2] = v;
             }
             __syncthreads();
         }
-        float *Out = Out0 + (long long)t * 2 * s.n4;
-        // tile (R, C): tmp_index(n, r_l, mu2, nu2 * 32 + c_l, part), fastest index mu1 = r_l
+        // tile (R, C): tmp_index(n, r_l, mu2, nu2 * 32 + c_l, part), fastest index mu1 = r_l;
+        // tile (C, R): element (c, r) = conj(v) at tmp_index(n, c_l, nu2, mu2 * 32 + r_l, part),
+        // fastest index nu1 = c_l (the lane), read transposed from the staging tile
+        float *Ot = t ? Out1 : Out0;
+        float *Orc = Ot + (mu2 * n2 + nu2 * kTB) * 2 * n + oo;
+        float *Ocr = Ot + (nu2 * n2 + mu2 * kTB) * 2 * n + oo;
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const int cl = w + 16 * j;
-            const float2 v = KF[cl * KLD + rl];
-            const int o = ((mu2 * n * n + nu2 * kTB + cl) * 2) * n + rl;
-            Out[o] = v.x;
-            Out[o + n] = v.y;
+            const float2 v = KF[ogT + 16 * KLD * j];
+            Orc[j * 16 * 2 * n] = v.x;
+            Orc[j * 16 * 2 * n + n] = v.y;
         }
         if (!diag) {
-            // tile (C, R): element (c, r) = conj(v) at tmp_index(n, c_l, nu2, mu2 * 32 + r_l, part),
-            // fastest index nu1 = c_l (the lane)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-                const int rr = w + 16 * j;
-                const float2 v = KF[rl * KLD + rr];
-                const int o = ((nu2 * n * n + mu2 * kTB + rr) * 2) * n + rl;
-                Out[o] = v.x;
-                Out[o + n] = -v.y;
+                const float2 v = KF[og11 + 16 * j];
+                Ocr[j * 16 * 2 * n] = v.x;
+                Ocr[j * 16 * 2 * n + n] = -v.y;
             }
         }
     }
