@@ -28,6 +28,10 @@
 namespace g12 {
 
 constexpr int kEpiPThreads = 512;
+constexpr int kEpiPWarps = kEpiPThreads / 32;
+constexpr int kEpiPEJ = kTB / kEpiPWarps;  // elements per thread and tile pair: (lane, w + kEpiPWarps j)
+constexpr int kEpiPChunks = 2 * kTB * kTB / 4;  // 16-byte chunks of one W tile
+static_assert(kEpiPChunks == 512 && (kEpiPThreads == 512 || kEpiPThreads == 1024), "chunk and element mapping");
 constexpr int kEpiPMaxUnits = 16;  // tile pairs per CTA (the host keeps the grid at >= 2 npairs / 16)
 
 struct EpiPBuf {
@@ -85,12 +89,15 @@ __device__ __forceinline__ void epip_issue_bulk(const SymDev &s, int k, const Ep
 }
 
 // every thread: its 16-byte chunk (source offset src, swizzled destination dst)
-// of both W tiles of a tile pair; Wt = W of the pair's tensor
+// of both W tiles of a tile pair (512 threads) or of one of them (1024 threads:
+// the first half the direct tile); Wt = W of the pair's tensor
 __device__ __forceinline__ void epip_issue_w(const float *Wt, const EpiPUnit &un, EpiPBuf &b, int dst, int src)
 {
     constexpr int n2 = 32 * 32;
-    cp_async16(&b.Wrc[dst], Wt + (2 * un.Cb * kTB) * n2 + un.Rb * kTB + src);
-    cp_async16(&b.Wcr[dst], Wt + (2 * un.Rb * kTB) * n2 + un.Cb * kTB + src);
+    if (kEpiPThreads == 512 || int(threadIdx.x) < kEpiPChunks)
+        cp_async16(&b.Wrc[dst], Wt + (2 * un.Cb * kTB) * n2 + un.Rb * kTB + src);
+    if (kEpiPThreads == 512 || int(threadIdx.x) >= kEpiPChunks)
+        cp_async16(&b.Wcr[dst], Wt + (2 * un.Rb * kTB) * n2 + un.Cb * kTB + src);
 }
 
 __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
@@ -106,7 +113,6 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     }
     constexpr int n = 32, n2 = n * n, GLD = n + 1, KLD = kTB + 1;
     constexpr int n3 = n * n * n;
-    static_assert(2 * kTB * kTB / 4 == kEpiPThreads, "one 16-byte chunk of each W tile per thread");
     extern __shared__ __align__(16) unsigned char smp[];
     double2 *Gs = reinterpret_cast<double2 *>(smp);  // n x GLD
     double2 *Ks = Gs + n * GLD;                       // [c_l][r_l] K of a diagonal pair, rows of KLD
@@ -115,7 +121,7 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     __shared__ int site[n];
     __shared__ double wtab[n];  // pair weight by site distance m: U (m = 0), V_m (m <= nv), 0
     __shared__ EpiPUnit units[kEpiPMaxUnits];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t bar[kEpiPEJ];
     const int tid = threadIdx.x;
     const int nu = (2 * s.npairs - int(blockIdx.x) + G - 1) / G;
     if (nu <= 0) return;
@@ -150,28 +156,29 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     }
     // Per-thread constants.  Copies: chunk cq of W tile row crho, 16-byte chunks
     // of a row swizzled: element (row rho, column c) at rho * 32 + ((((c >> 2) ^
-    // (rho >> 1)) & 7) << 2) + (c & 3).  Reads: element (r_l, c_l) = (lane, w + 16 j),
+    // (rho >> 1)) & 7) << 2) + (c & 3).  Reads: element (r_l, c_l) = (lane, w + kEpiPWarps j),
     // e = c_l * 32 + r_l; its W offsets in the direct tile (rho = 2 c_l + part,
     // c = r_l) and the transposed tile (rho = 2 r_l + part, c = c_l) do not depend
     // on the pair.
-    const int crho = tid >> 3, cq = tid & 7;
+    const int crho = (tid % kEpiPChunks) >> 3, cq = tid & 7;
     const int wdst = crho * kTB + (((cq ^ (crho >> 1)) & 7) << 2), wsrc = crho * n2 + 4 * cq;
     const int rl = tid & 31, w = tid >> 5;
     const int ow1 = 2 * w * kTB + ((((rl >> 2) ^ w) & 7) << 2) + (rl & 3);
-    const int ow2[2] = {2 * rl * kTB + ((((w >> 2) ^ rl) & 7) << 2) + (w & 3),
-                        2 * rl * kTB + (((((w >> 2) + 4) ^ rl) & 7) << 2) + (w & 3)};
-    const int e0 = w * kTB + rl;    // element j = 0 (j = 1: + 512)
-    const int og11 = rl * GLD + w;  // Gs[mu1][c_l] (j = 1: + 16); also KF / Ks at row r_l, column c_l
-    const int ogT = w * GLD + rl;   // Gs[c_l][mu1] (j = 1: + 16 GLD); also KF / Ks at row c_l, column r_l
-    const int oo = w * 2 * n + rl;  // output offset inside a tile's rows (j = 1: + 16 * 2n)
+    int ow2[kEpiPEJ];
+#pragma unroll
+    for (int j = 0; j < kEpiPEJ; ++j) ow2[j] = 2 * rl * kTB + (((((w + kEpiPWarps * j) >> 2) ^ rl) & 7) << 2) + (w & 3);
+    const int e0 = w * kTB + rl;    // element j = 0 (j: + kEpiPWarps 32 j)
+    const int og11 = rl * GLD + w;  // Gs[mu1][c_l] (j: + kEpiPWarps j); also KF / Ks at row r_l, column c_l
+    const int ogT = w * GLD + rl;   // Gs[c_l][mu1] (j: + kEpiPWarps GLD j); also KF / Ks at row c_l, column r_l
+    const int oo = w * 2 * n + rl;  // output offset inside a tile's rows (j: + kEpiPWarps 2n j)
     const float *Wt0 = s.W, *Wt1 = s.W + 2 * s.n4;
     float *const Out0 = sym_out<float>(s, k), *const Out1 = Out0 + 2 * s.n4;
     const int mu1 = rl;
     __syncthreads();
     const int si = site[mu1];
-    int sk[2];
-    sk[0] = site[w];
-    sk[1] = site[w + 16];
+    int sk[kEpiPEJ];
+#pragma unroll
+    for (int j = 0; j < kEpiPEJ; ++j) sk[j] = site[w + kEpiPWarps * j];
     // W comes from the GEMM launched just before this kernel, the tables from
     // k_prep before it (G1 was complete before k_prep started)
     grid_dep_wait();
@@ -221,28 +228,28 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         }
         const double dmu = U * double(mu1 == mu2);
         // loads of both elements first (the stores below go to other buffers)
-        double2 C[2], g11[2], gT[2], zd[2], acs[2], ycs[2];
-        double wb[2];
-        double2 rb[2], qb[2];
+        double2 C[kEpiPEJ], g11[kEpiPEJ], gT[kEpiPEJ], zd[kEpiPEJ], acs[kEpiPEJ], ycs[kEpiPEJ];
+        double wb[kEpiPEJ];
+        double2 rb[kEpiPEJ], qb[kEpiPEJ];
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int e = e0 + j * 16 * kTB;
-            const float w1x = b.Wrc[ow1 + j * 32 * kTB], w1y = b.Wrc[ow1 + j * 32 * kTB + kTB];
+        for (int j = 0; j < kEpiPEJ; ++j) {
+            const int e = e0 + j * kEpiPWarps * kTB;
+            const float w1x = b.Wrc[ow1 + j * 2 * kEpiPWarps * kTB], w1y = b.Wrc[ow1 + j * 2 * kEpiPWarps * kTB + kTB];
             const float w2x = b.Wcr[ow2[j]], w2y = b.Wcr[ow2[j] + kTB];
             C[j] = make_double2(double(w1x) - double(w2x), double(w1y) + double(w2y));
-            g11[j] = Gs[og11 + 16 * j];
-            gT[j] = Gs[ogT + 16 * GLD * j];
+            g11[j] = Gs[og11 + kEpiPWarps * j];
+            gT[j] = Gs[ogT + kEpiPWarps * GLD * j];
             zd[j] = diag ? make_double2(0.0, 0.0) : c_sub(b.Zm[e], b.Zn[e]);
             acs[j] = b.Ac[e];
             ycs[j] = b.Yc[e];
             wb[j] = wtab[abs(sk[j] - sl)];
             rb[j] = b.Rt[sk[j]];
-            qb[j] = b.Qr[w + 16 * j];
+            qb[j] = b.Qr[w + kEpiPWarps * j];
         }
-        double2 Kv[2];
+        double2 Kv[kEpiPEJ];
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int nu1 = w + 16 * j;
+        for (int j = 0; j < kEpiPEJ; ++j) {
+            const int nu1 = w + kEpiPWarps * j;
             const double2 g1122 = c_mul(g11[j], g22);
             double2 psi = c_scale(g1122, wa - wb[j]);
             psi = c_add(psi, c_i(c_mul(g11[j], c_sub(ra, rb[j]))));
@@ -274,30 +281,30 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         };
         if (!diag) {
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const double2 v = rk4(Kv[j], acs[j], ycs[j], e0 + j * 16 * kTB);
-                KF[ogT + 16 * KLD * j] = make_float2(float(v.x), float(v.y));
+            for (int j = 0; j < kEpiPEJ; ++j) {
+                const double2 v = rk4(Kv[j], acs[j], ycs[j], e0 + j * kEpiPWarps * kTB);
+                KF[ogT + kEpiPWarps * KLD * j] = make_float2(float(v.x), float(v.y));
             }
             __syncthreads();
         } else {
             // keep the diagonal block exactly Hermitian: K <- (K + K^H) / 2, then the
             // bookkeeping and the particle-2 diagonal D (mu2 == nu2 on these pairs)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) Ks[ogT + 16 * KLD * j] = Kv[j];
+            for (int j = 0; j < kEpiPEJ; ++j) Ks[ogT + kEpiPWarps * KLD * j] = Kv[j];
             __syncthreads();
-            double2 sym[2];
+            double2 sym[kEpiPEJ];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const double2 a = Ks[ogT + 16 * KLD * j], bb = c_conj(Ks[og11 + 16 * j]);
+            for (int j = 0; j < kEpiPEJ; ++j) {
+                const double2 a = Ks[ogT + kEpiPWarps * KLD * j], bb = c_conj(Ks[og11 + kEpiPWarps * j]);
                 sym[j] = make_double2(0.5 * (a.x + bb.x), 0.5 * (a.y + bb.y));
             }
             __syncthreads();
             double2 *Dt = d.D + t * n3;
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const double2 v = rk4(sym[j], acs[j], ycs[j], e0 + j * 16 * kTB);
-                KF[ogT + 16 * KLD * j] = make_float2(float(v.x), float(v.y));
-                Dt[(mu1 * n + w + 16 * j) * n + mu2] = v;
+            for (int j = 0; j < kEpiPEJ; ++j) {
+                const double2 v = rk4(sym[j], acs[j], ycs[j], e0 + j * kEpiPWarps * kTB);
+                KF[ogT + kEpiPWarps * KLD * j] = make_float2(float(v.x), float(v.y));
+                Dt[(mu1 * n + w + kEpiPWarps * j) * n + mu2] = v;
             }
             __syncthreads();
         }
@@ -308,17 +315,17 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
         float *Orc = Ot + (mu2 * n2 + nu2 * kTB) * 2 * n + oo;
         float *Ocr = Ot + (nu2 * n2 + mu2 * kTB) * 2 * n + oo;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const float2 v = KF[ogT + 16 * KLD * j];
-            Orc[j * 16 * 2 * n] = v.x;
-            Orc[j * 16 * 2 * n + n] = v.y;
+        for (int j = 0; j < kEpiPEJ; ++j) {
+            const float2 v = KF[ogT + kEpiPWarps * KLD * j];
+            Orc[j * kEpiPWarps * 2 * n] = v.x;
+            Orc[j * kEpiPWarps * 2 * n + n] = v.y;
         }
         if (!diag) {
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const float2 v = KF[og11 + 16 * j];
-                Ocr[j * 16 * 2 * n] = v.x;
-                Ocr[j * 16 * 2 * n + n] = -v.y;
+            for (int j = 0; j < kEpiPEJ; ++j) {
+                const float2 v = KF[og11 + kEpiPWarps * j];
+                Ocr[j * kEpiPWarps * 2 * n] = v.x;
+                Ocr[j * kEpiPWarps * 2 * n + n] = -v.y;
             }
         }
     }
