@@ -295,9 +295,17 @@ def full_run_error(g12, p, S, precision, local):
     for prec in ("fp64", precision):
         with g12.Context(p, prec, local) as ctx:
             ctx.set_state(*S)
+            ctx.propagate(8)  # graph capture outside the timed call
+            ctx.set_state(*S)
+            t0 = time.perf_counter()
             tr, rc = ctx.propagate(T)
+            wall = time.perf_counter() - t0
             out[prec + "_status"] = rc
             out[prec + "_device_s"] = ctx.last_device_ms / 1e3
+            # the G1 snapshot of every step (T x n^2 complex) comes back during the call:
+            # each finished half of the device ring is copied while the next half runs
+            out[prec + "_call_wall_s"] = wall
+            out[prec + "_snapshot_bytes"] = int(tr.nbytes)
         trajs[prec] = tr
     ref, got = trajs["fp64"], trajs[precision]
     out["g1_max_rel_err"] = float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))

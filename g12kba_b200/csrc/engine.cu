@@ -51,6 +51,12 @@ struct g12_ctx {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // snapshot copies of a finished half of the trajectory ring, overlapped with
+    // the next half's steps: copy stream, per-half events (start and end of the
+    // half's steps, end of its copy) and the guard status after each half (pinned)
+    cudaStream_t s_copy = nullptr;
+    cudaEvent_t ev_hs[2] = {}, ev_he[2] = {}, ev_hc[2] = {};
+    int *status_h = nullptr;
     StepP *sched_dev = nullptr;
     long long sched_cap = 0;
     StepP *sched_host = nullptr;  // pinned
@@ -284,6 +290,81 @@ int build_graph(g12_ctx *ctx)
 
 // Runs `steps` scheduled steps (already in sched_host) through the graph.
 // traj_out / dip_out (host, nullable) receive one entry per recorded step.
+// The steps in halves of the snapshot ring: while half h's steps run, the
+// previous half's snapshots and dipoles are copied to the caller's buffers on
+// the copy stream; a half's steps wait (on the device) for the copy of the
+// half that used the same ring slots two halves earlier.  The guard status is
+// read after each half (pinned word); a tripped guard ends the call there.
+int run_steps_overlapped(g12_ctx *ctx, long long steps, double *traj_out, double *dip_out, bool recorded,
+                         long long *done)
+{
+    const long long G = ctx->lc.steps_per_graph;
+    const long long half = std::max<long long>(G, (ctx->traj_cap / 2) / G * G);
+    CK(cudaMemcpyAsync(ctx->d.limit, &steps, sizeof(long long), cudaMemcpyHostToDevice, ctx->s));
+    const long long nh = (steps + half - 1) / half;
+    float total_ms = 0;
+    // finish half c: its status, its time, its copies
+    auto finish = [&](long long c, long long *got_out) -> int {
+        const int h = int(c & 1);
+        const long long b = c * half, len = std::min(half, steps - b);
+        CK(cudaEventSynchronize(ctx->ev_he[h]));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev_hs[h], ctx->ev_he[h]);
+        total_ms += ms;
+        const int status = ctx->status_h[h];
+        long long got = len;
+        if (status > 0) got = std::min(len, (long long)status - b);  // guard at step status-1
+        if (recorded && got > 0) {
+            const long long off = b % ctx->traj_cap;
+            CK(cudaStreamWaitEvent(ctx->s_copy, ctx->ev_he[h], 0));
+            if (traj_out)
+                CK(cudaMemcpyAsync(traj_out + 2 * b * ctx->n2, ctx->d.traj + off * ctx->n2,
+                                   got * ctx->n2 * sizeof(double2), cudaMemcpyDeviceToHost, ctx->s_copy));
+            if (dip_out)
+                CK(cudaMemcpyAsync(dip_out + b, ctx->d.dip + off, got * sizeof(double), cudaMemcpyDeviceToHost,
+                                   ctx->s_copy));
+        }
+        CK(cudaEventRecord(ctx->ev_hc[h], ctx->s_copy));
+        if (ctx->prec != G12_PREC_FP64) {
+            const int me = mixed_error(ctx->mixed);
+            if (me) {
+                ctx->err = "tensor-core pipeline wait expired (code " + std::to_string(me) + ")";
+                return G12_ERR_CUDA;
+            }
+        }
+        *got_out = got;
+        return status > 0 ? G12_GUARD_TRIPPED : G12_OK;
+    };
+    long long base = 0;
+    int rc = G12_OK;
+    for (long long c = 0; c < nh && rc == G12_OK; ++c) {
+        const int h = int(c & 1);
+        const long long len = std::min(half, steps - c * half);
+        // ring slots of this half: free once the copy of half c - 2 is done
+        if (c >= 2) CK(cudaStreamWaitEvent(ctx->s, ctx->ev_hc[h], 0));
+        CK(cudaEventRecord(ctx->ev_hs[h], ctx->s));
+        for (long long q = 0; q < len; q += G) CK(cudaGraphLaunch(ctx->graph, ctx->s));
+        CK(cudaMemcpyAsync(&ctx->status_h[h], ctx->d.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->s));
+        CK(cudaEventRecord(ctx->ev_he[h], ctx->s));
+        if (c >= 1) {
+            long long got = 0;
+            rc = finish(c - 1, &got);
+            base += got;
+        }
+    }
+    if (rc == G12_OK) {
+        long long got = 0;
+        rc = finish(nh - 1, &got);
+        base += got;
+    }
+    // a tripped guard leaves the queued half inert (its steps return at once)
+    CK(cudaStreamSynchronize(ctx->s));
+    CK(cudaStreamSynchronize(ctx->s_copy));
+    *done = base;
+    ctx->last_ms = total_ms;
+    return rc;
+}
+
 int run_steps(g12_ctx *ctx, long long steps, double *traj_out, double *dip_out, long long *done)
 {
     *done = 0;
@@ -297,6 +378,8 @@ int run_steps(g12_ctx *ctx, long long steps, double *traj_out, double *dip_out, 
     const bool recorded = ctx->sched_host[0].record != 0;
     float total_ms = 0;
     long long base = 0;
+    if (!ctx->evict_bytes && ctx->traj_cap >= 2 * ctx->lc.steps_per_graph)
+        return run_steps_overlapped(ctx, steps, traj_out, dip_out, recorded, done);
     while (base < steps) {
         const long long chunk = std::min(steps - base, ctx->traj_cap);
         const long long lim = base + chunk;
@@ -430,6 +513,14 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
         return fail(G12_ERR_CUDA);
     cudaEventCreate(&ctx->ev0);
     cudaEventCreate(&ctx->ev1);
+    if (!ck(ctx, cudaStreamCreateWithFlags(&ctx->s_copy, cudaStreamNonBlocking), "cudaStreamCreate") ||
+        !ck(ctx, cudaMallocHost(&ctx->status_h, 2 * sizeof(int)), "cudaMallocHost"))
+        return fail(G12_ERR_CUDA);
+    for (int h = 0; h < 2; ++h)
+        if (!ck(ctx, cudaEventCreate(&ctx->ev_hs[h]), "cudaEventCreate") ||
+            !ck(ctx, cudaEventCreate(&ctx->ev_he[h]), "cudaEventCreate") ||
+            !ck(ctx, cudaEventCreateWithFlags(&ctx->ev_hc[h], cudaEventDisableTiming), "cudaEventCreate"))
+            return fail(G12_ERR_CUDA);
 
     Dev &d = ctx->d;
     d.Ns = p->Ns;
@@ -515,6 +606,14 @@ extern "C" int g12_destroy(g12_ctx *ctx)
     if (ctx->sched_host) cudaFreeHost(ctx->sched_host);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->s_copy) cudaStreamSynchronize(ctx->s_copy);
+    for (int h = 0; h < 2; ++h) {
+        if (ctx->ev_hs[h]) cudaEventDestroy(ctx->ev_hs[h]);
+        if (ctx->ev_he[h]) cudaEventDestroy(ctx->ev_he[h]);
+        if (ctx->ev_hc[h]) cudaEventDestroy(ctx->ev_hc[h]);
+    }
+    if (ctx->status_h) cudaFreeHost(ctx->status_h);
+    if (ctx->s_copy) cudaStreamDestroy(ctx->s_copy);
     for (cudaEvent_t e : ctx->ring) cudaEventDestroy(e);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
     if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);

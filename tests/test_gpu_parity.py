@@ -215,6 +215,51 @@ def test_device_dipole_and_chunked_clock(g12):
     assert rel_err(dip, g["dipole"]) <= RUN_TOL
 
 
+def test_snapshot_ring_halves_split_calls_bitwise(g12):
+    """One call over several halves of the snapshot ring (copies overlapped with
+    the next half's steps) equals the same steps taken in uneven calls."""
+    p = g12.make_params(Ns=4, Nb=2, Nq=2, time_steps=10000, U=1.0, t2=0.2, EHM=True, dt=0.02)
+    G0 = g12.make_G0(p)
+    with g12.Context(p) as ctx:
+        ctx.set_state(G0)
+        ctx.adiabatic_switch()
+        S = ctx.get_state()
+        traj, rc = ctx.propagate(5000)
+        end = ctx.get_state()
+    assert rc == 0 and traj.shape[0] == 5000
+    parts = []
+    with g12.Context(p) as ctx:
+        ctx.set_state(*S)
+        for m in (1, 2047, 2050, 902):
+            t, rc = ctx.propagate(m)
+            assert rc == 0
+            parts.append(t)
+        end2 = ctx.get_state()
+    assert np.array_equal(traj, np.concatenate(parts))
+    for a, b in zip(end, end2):
+        assert np.array_equal(a, b)
+
+
+def test_guard_trip_with_a_later_half_queued(g12):
+    """The guard trips in the first half of a call that spans several halves:
+    the call stops there, the queued half leaves the state alone."""
+    g = load_golden("run_guard.npz")
+    cfg = _cfg_from(g)
+    p = params_of(g12, cfg)
+    p.time_steps = 6000  # same schedule for the first steps, several ring halves
+    T = int(g["T"])
+    with g12.Context(p) as ctx:
+        ctx.set_state(g["g0"])
+        ctx.adiabatic_switch()
+        traj, rc = ctx.propagate(g12.rk_iterations(p))
+        G1 = ctx.get_state()[0]
+    assert g12.rk_iterations(p) > 4100
+    assert rc == g12.G12_GUARD_TRIPPED and traj.shape[0] == T
+    assert rel_err(traj[:-1], g["traj"][:-1]) <= RUN_TOL
+    # the state stays at the recorded offending snapshot: the queued half did not advance it
+    assert np.array_equal(G1, traj[-1])
+
+
 def test_deterministic(g12):
     g = load_golden("run_ehm_nb2.npz")
     p = params_of(g12, _cfg_from(g))
