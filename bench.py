@@ -49,9 +49,9 @@ EVICT_BYTES = 160 << 20
 # DRAM bytes (read + write) per launch of the top kernels at n = 32, from one
 # `ncu --set full` capture each (the profiles/ summaries give the command).
 TOP_KERNEL_DRAM_BYTES = {
-    "k_sym_gemm_oz2": 16863232.0,
-    "k_sym_epi": 37610752.0,
-    "k_apply<cols+epilogue>": 95704832.0,
+    "k_sym_gemm_oz2": 16860928.0,
+    "k_sym_epi": 36916480.0,
+    "k_apply_tc<cols+epilogue>": 170896896.0,
 }
 
 # Algorithmic HBM bytes per launch in units of n^4 (both G2 tensors):
