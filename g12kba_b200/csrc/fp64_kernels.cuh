@@ -503,8 +503,9 @@ struct ApplyEpi {
     {
         const int n = d.n, Ns = d.Ns;
         U = st.U;
-        mu1 = int(r % n);
-        mu2 = int(r / n);
+        const int ri = int(r_);  // a row of M: r < n^2
+        mu1 = ri % n;
+        mu2 = ri / n;
         si = mu1 % Ns;
         sj = mu2 % Ns;
         wij = U * double(si == sj) + vdist(d, si, sj);
@@ -660,20 +661,25 @@ __device__ __forceinline__ void apply_body(const Dev &d, int k, const ApplyCfg &
         return;
     }
 
-    if (!live) return;
-    // ---- fused epilogue (CD) ----
+    // ---- fused epilogue (CD): Y through shared memory, then one element per
+    // thread with consecutive threads on consecutive elements (nu1 fastest), so
+    // the element's global reads and writes run along rows of M
+    __syncthreads();
+    if (live) {
+        double2 *Ym = Xs + (size_t)mat * NP * LD;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) Ym[(ti + S * a) * LD + tj + S * b] = acc[a][b];
+    }
+    __syncthreads();
     const StageP st = d.cur->st[k];
-    const ApplyEpi ep(d, st, m0 + mat);
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const int nu2 = ti + S * a;
-        if (nu2 >= n) continue;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int nu1 = tj + S * b;
-            if (nu1 >= n) continue;
-            ep.element(d, k, t, nu1, nu2, acc[a][b], Gs, n);
-        }
+    const int n2i = n * n;
+    for (int e = threadIdx.x; e < nm * n2i; e += blockDim.x) {
+        const int rb = e / n2i, c = e - rb * n2i;
+        const int nu1 = c % n, nu2 = c / n;
+        const ApplyEpi ep(d, st, m0 + rb);
+        ep.element(d, k, t, nu1, nu2, Xs[(size_t)rb * NP * LD + nu2 * LD + nu1], Gs, n);
     }
 }
 
