@@ -383,7 +383,7 @@ int autotune_tc(g12_batch *b, int sys)
     const int n = d.n;
     size_t sab = 0, scd = 0;
     const ApplyTcCfg base = make_apply_tc_cfg(n, &sab, &scd);
-    const int tpm = (base.NP / 16) * (base.NP / 16);
+    const int tpm = apply_tc_tpm(base);
     std::vector<int> cands;
     for (int nb = 1; nb * tpm * 32 <= kTcThreads && nb <= n * n; nb *= 2) {
         tc_cfg_nb(n, nb, &sab, &scd);
@@ -400,14 +400,14 @@ int autotune_tc(g12_batch *b, int sys)
     for (int nb : cands) {
         const ApplyTcCfg c = tc_cfg_nb(n, nb, &sab, &scd);
         const dim3 grid(unsigned((d.n2 + nb - 1) / nb), 2);
-        cudaFuncSetAttribute(k_apply_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sab));
-        cudaFuncSetAttribute(k_apply_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(scd));
+        apply_tc_smem_attr<false>(c, sab);
+        apply_tc_smem_attr<true>(c, scd);
         Dev dd = d;
         dd.debug = 1;  // results go to the scratch tensors only
         for (int rep = 0; rep < 4; ++rep) {
             cudaEventRecord(b->ev0, b->s);
-            k_apply_tc<false><<<grid, kTcThreads, sab, b->s>>>(dd, 0, c);
-            k_apply_tc<true><<<grid, kTcThreads, scd, b->s>>>(dd, 0, c);
+            launch_apply_tc<false>(grid, sab, b->s, dd, 0, c);
+            launch_apply_tc<true>(grid, scd, b->s, dd, 0, c);
             cudaEventRecord(b->ev1, b->s);
             cudaEventSynchronize(b->ev1);
             float ms = 0;

@@ -222,8 +222,8 @@ int ensure_sched(g12_ctx *ctx, long long steps)
 void enqueue_apply(const LaunchCfg &lc, const Dev &d, int k, cudaStream_t s, int q = -1)
 {
     if (lc.tc) {
-        if (q != 1) k_apply_tc<false><<<lc.tc_grid, lc.tcc.threads, lc.tc_ab_smem, s>>>(d, k, lc.tcc);
-        if (q != 0) k_apply_tc<true><<<lc.tc_grid, lc.tcc.threads, lc.tc_cd_smem, s>>>(d, k, lc.tcc);
+        if (q != 1) launch_apply_tc<false>(lc.tc_grid, lc.tc_ab_smem, s, d, k, lc.tcc);
+        if (q != 0) launch_apply_tc<true>(lc.tc_grid, lc.tc_cd_smem, s, d, k, lc.tcc);
     } else {
         if (q != 1) k_apply<false><<<lc.apply_grid, lc.ab_threads, lc.ab_smem, s>>>(d, k, lc.ab);
         if (q != 0) k_apply<true><<<lc.apply_grid, lc.cd_threads, lc.cd_smem, s>>>(d, k, lc.cd);
@@ -568,8 +568,8 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     if (lc.tc) {
         lc.tcc = make_apply_tc_cfg(n, &lc.tc_ab_smem, &lc.tc_cd_smem);
         lc.tc_grid = dim3(unsigned((n2 + lc.tcc.NB - 1) / lc.tcc.NB), 2, 1);
-        if (!ck(ctx, cudaFuncSetAttribute(k_apply_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.tc_ab_smem)), "attr") ||
-            !ck(ctx, cudaFuncSetAttribute(k_apply_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.tc_cd_smem)), "attr"))
+        if (!ck(ctx, apply_tc_smem_attr<false>(lc.tcc, lc.tc_ab_smem), "attr") ||
+            !ck(ctx, apply_tc_smem_attr<true>(lc.tcc, lc.tc_cd_smem), "attr"))
             return fail(G12_ERR_CUDA);
     }
     if (!ck(ctx, cudaFuncSetAttribute(k_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.ab_smem)), "attr") ||

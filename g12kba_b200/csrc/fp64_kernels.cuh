@@ -690,18 +690,26 @@ static __global__ void __launch_bounds__(256) k_apply(Dev d, int k, ApplyCfg cfg
 }
 
 // FP64 tensor-core version of the two halves (n = 16 .. 48): mma.sync
-// m8n8k4 f64 (DMMA).  Each warp computes a 16 x 16 complex block of
-// Y = L X + X R for one matrix (2 x 2 tiles of 8 x 8, real and imaginary parts,
-// 4 real products per complex product, accumulated in FP64 like the FMA
-// path).  Operands live in shared memory as separate real and imaginary
-// planes of NP x LDD doubles, NP = n rounded up to 16 (zero padding), LDD = 12
-// mod 16, so the fragment loads of the row-major A and column-major B operands
-// touch each 8-byte bank at most twice per warp.  Results return through the
+// m8n8k4 f64 (DMMA).  Each warp computes an 8 BI x 8 BJ complex block of
+// Y = L X + X R for one matrix (BI x BJ tiles of 8 x 8, real and imaginary
+// parts, 4 real products per complex product, accumulated in FP64 like the FMA
+// path): kind B = 3 is NP = 24 with 1 x 3 tiles per warp (three warps per
+// matrix, for 16 < n <= 24), kind B = 2 is NP = n rounded up to 16 with 2 x 2
+// tiles (zero padding either way).  Operands live in shared memory
+// as separate real and imaginary planes of NP x LDD doubles, LDD = 12 mod 16,
+// so the fragment loads of the row-major A and column-major B operands touch
+// each 8-byte bank at most twice per warp.  Results return through the
 // X planes; the column half then runs the same per-element epilogue
 // (ApplyEpi) as the FMA path, with consecutive threads on consecutive nu1.
 struct ApplyTcCfg {
-    int NP, LDD, NB, threads;
+    int NP, LDD, NB, threads, B;
 };
+
+// warps per matrix: (NP / 8 BI) x (NP / 8 BJ); kind 3: BI = 1, BJ = 3, kind 2: BI = BJ = 2
+__host__ __device__ inline int apply_tc_tpm(const ApplyTcCfg &c)
+{
+    return c.B == 3 ? (c.NP / 8) * (c.NP / 24) : (c.NP / 16) * (c.NP / 16);
+}
 
 inline bool apply_tc_ok(int n) { return n >= 16 && n <= 48; }
 
@@ -713,11 +721,13 @@ __host__ __device__ inline int apply_tc_plane(int NP, int LDD) { return NP * LDD
 inline ApplyTcCfg make_apply_tc_cfg(int n, size_t *smem_ab, size_t *smem_cd)
 {
     ApplyTcCfg c;
-    c.NP = (n + 15) / 16 * 16;
-    c.LDD = c.NP + 12;
-    const int tpm = (c.NP / 16) * (c.NP / 16);
+    const bool b3 = n > 16 && n <= 24;
+    c.B = b3 ? 3 : 2;
+    c.NP = b3 ? 24 : (n + 15) / 16 * 16;
+    c.LDD = b3 ? 28 : c.NP + 12;
+    const int tpm = apply_tc_tpm(c);
     const size_t plane = size_t(apply_tc_plane(c.NP, c.LDD)) * sizeof(double);
-    c.NB = std::max(1, std::min(n * n, 8 / tpm));  // 2 matrices per block at n = 32 (6% faster than 4)
+    c.NB = std::max(1, std::min(n * n, (c.B == 3 ? 15 : 8) / tpm));  // 2 matrices per block at n = 32 (6% faster than 4)
     while (c.NB > 1 && (4 + 2 * size_t(c.NB)) * plane + size_t(n) * (n + 1) * sizeof(double2) > 200 * 1024) c.NB--;
     c.threads = c.NB * tpm * 32;
     *smem_ab = (4 + 2 * size_t(c.NB)) * plane;
@@ -732,8 +742,8 @@ __device__ __forceinline__ void dmma_f64(double &c0, double &c1, double a, doubl
                  : "d"(a), "d"(b));
 }
 
-template <bool CD>
-__device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTcCfg &cfg, int bx, int t)
+template <bool CD, int BI, int BJ>
+__device__ __forceinline__ void apply_tc_body_b(const Dev &d, int k, const ApplyTcCfg &cfg, int bx, int t)
 {
     if (!*d.active) return;
     const int n = d.n, NP = cfg.NP, LDD = cfg.LDD, NB = cfg.NB;
@@ -791,37 +801,37 @@ __device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTc
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-    const int TW = NP / 16, tpm = TW * TW;
+    const int TWI = NP / (8 * BI), TWJ = NP / (8 * BJ), tpm = TWI * TWJ;
     const int mat = warp / tpm, wt = warp % tpm;
-    const int row0 = (wt / TW) * 16, col0 = (wt % TW) * 16;
+    const int row0 = (wt / TWJ) * 8 * BI, col0 = (wt % TWJ) * 8 * BJ;
     const bool live = mat < nm;
-    double yr[2][2][2], yi[2][2][2];
+    double yr[BI][BJ][2], yi[BI][BJ][2];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < BI; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j)
+        for (int j = 0; j < BJ; ++j)
 #pragma unroll
             for (int q = 0; q < 2; ++q) yr[i][j][q] = yi[i][j][q] = 0.0;
     if (live) {
         const double *Xr = Xp + 2 * mat * PL, *Xi = Xr + PL;
         auto step = [&](const double *Ar, const double *Ai, const double *Br, const double *Bi, int k0) {
-            double ar[2], ai[2], br[2], bi[2];
+            double ar[BI], ai[BI], br[BJ], bi[BJ];
 #pragma unroll
-            for (int i = 0; i < 2; ++i) {
+            for (int i = 0; i < BI; ++i) {
                 const int o = (row0 + 8 * i + gid) * LDD + k0 + tig;
                 ar[i] = Ar[o];
                 ai[i] = Ai[o];
             }
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
+            for (int j = 0; j < BJ; ++j) {
                 const int o = (k0 + tig) * LDD + col0 + 8 * j + gid;
                 br[j] = Br[o];
                 bi[j] = Bi[o];
             }
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
+            for (int i = 0; i < BI; ++i)
 #pragma unroll
-                for (int j = 0; j < 2; ++j) {
+                for (int j = 0; j < BJ; ++j) {
                     dmma_f64(yr[i][j][0], yr[i][j][1], ar[i], br[j]);
                     dmma_f64(yr[i][j][0], yr[i][j][1], -ai[i], bi[j]);
                     dmma_f64(yi[i][j][0], yi[i][j][1], ar[i], bi[j]);
@@ -837,9 +847,9 @@ __device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTc
     if (live) {
         double *Yr = Xp + 2 * mat * PL, *Yi = Yr + PL;
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < BI; ++i)
 #pragma unroll
-            for (int j = 0; j < 2; ++j)
+            for (int j = 0; j < BJ; ++j)
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     const int o = (row0 + 8 * i + gid) * LDD + col0 + 8 * j + 2 * tig + q;
@@ -871,10 +881,34 @@ __device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTc
     }
 }
 
+// the body for the configuration's B (uniform branch; the batch kernel serves
+// systems of both kinds)
 template <bool CD>
+__device__ __forceinline__ void apply_tc_body(const Dev &d, int k, const ApplyTcCfg &cfg, int bx, int t)
+{
+    if (cfg.B == 3) apply_tc_body_b<CD, 1, 3>(d, k, cfg, bx, t);
+    else apply_tc_body_b<CD, 2, 2>(d, k, cfg, bx, t);
+}
+
+template <bool CD, int B>
 static __global__ void __launch_bounds__(512) k_apply_tc(Dev d, int k, ApplyTcCfg cfg)
 {
-    apply_tc_body<CD>(d, k, cfg, blockIdx.x, blockIdx.y);
+    apply_tc_body_b<CD, B == 3 ? 1 : 2, B == 3 ? 3 : 2>(d, k, cfg, blockIdx.x, blockIdx.y);
+}
+
+// launch of the DMMA half CD with the kernel instance of cfg.B
+template <bool CD>
+inline void launch_apply_tc(dim3 grid, size_t smem, cudaStream_t s, const Dev &d, int k, const ApplyTcCfg &cfg)
+{
+    if (cfg.B == 3) k_apply_tc<CD, 3><<<grid, cfg.threads, smem, s>>>(d, k, cfg);
+    else k_apply_tc<CD, 2><<<grid, cfg.threads, smem, s>>>(d, k, cfg);
+}
+
+template <bool CD>
+inline cudaError_t apply_tc_smem_attr(const ApplyTcCfg &cfg, size_t smem)
+{
+    return cfg.B == 3 ? cudaFuncSetAttribute(k_apply_tc<CD, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))
+                      : cudaFuncSetAttribute(k_apply_tc<CD, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
 }
 
 // D[t][a][b][r] = Y2_t[a, r; b, r]
