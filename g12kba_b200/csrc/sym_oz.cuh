@@ -164,7 +164,8 @@ __device__ __forceinline__ void named_sync(int id, int nthreads)
 // Roles (26 warps at n = 32, 18 at n = 16):
 //   warp 0      TMA producer: FP32 A tiles into a 2-stage ring (starts as soon
 //               as the barriers exist)
-//   warp 1      one thread issues the 10 digit products per tile into one of
+//   warp 1      one thread issues the digit products per tile (one per input
+//               digit i, against digits 0 .. 3 - i of h at once) into one of
 //               two TMEM accumulator sets
 //   warps 2-9   digit split, two threads per A row (row max, exponent, 4 bf16
 //               digit rows)
@@ -220,6 +221,7 @@ struct Oz2Shape {
     static constexpr int OFF_BAR = OFF_L + 2 * kOz2ListTiles * CPT * 4;
     static constexpr int SMEM = OFF_BAR + 16 * 8 + 1024;
     static_assert(kOz2Digits * N <= ACC, "accumulator set");
+    static_assert(kOz2Digits * N <= 256 && N % 16 == 0, "one product spans the digit tiles of h (UMMA N <= 256)");
     static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
@@ -323,7 +325,6 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                     ok = false;
                     atomicExch(s.err, 8);
                 }
-                const uint32_t idesc = umma_idesc_bf16(Sh::N);
                 const uint32_t bb = smem_u32(Bd);
                 int done = 0;
                 for (int i = 0; i < my_tiles && ok; ++i) {
@@ -336,16 +337,16 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                     tc_fence_after();
                     const uint32_t ab = smem_u32(Ds + db * Sh::D_SET);
                     const uint32_t acc0 = tmem + b * Sh::ACC;
-                    for (int L = 0; L < kOz2Digits; ++L) {
-                        uint32_t acc = 0;
-                        for (int ii = 0; ii <= L; ++ii) {
-                            const int jj = L - ii;
-                            for (int ks = 0; ks < Sh::KS; ++ks) {
-                                umma_bf16(acc0 + L * Sh::N, umma_desc_sw128(ab + ii * Sh::D_BYTES + ks * 32),
-                                          umma_desc_sw128(bb + jj * Sh::B_BYTES + ks * 32), idesc, acc);
-                                acc = 1;
-                            }
-                        }
+                    // digit ii of the input times digits 0 .. 3 - ii of h in one product:
+                    // the digit tiles of h are consecutive rows of one operand and the
+                    // levels ii .. 3 consecutive accumulator columns, so level L receives
+                    // A_ii B_(L - ii) for ii = 0 .. L in this order (each A digit tile is
+                    // read once per K step instead of once per level)
+                    for (int ii = 0; ii < kOz2Digits; ++ii) {
+                        const uint32_t idesc = umma_idesc_bf16((kOz2Digits - ii) * Sh::N);
+                        for (int ks = 0; ks < Sh::KS; ++ks)
+                            umma_bf16(acc0 + ii * Sh::N, umma_desc_sw128(ab + ii * Sh::D_BYTES + ks * 32),
+                                      umma_desc_sw128(bb + ks * 32), idesc, (ii > 0 || ks > 0) ? 1u : 0u);
                     }
                     umma_commit(&acc_full[b]);
                     umma_commit(&dig_empty[db]);
