@@ -4,11 +4,13 @@
 // for the B200 memory system instead of one short-lived block per tile pair:
 //   * one 512-thread CTA per SM walks its tile pairs (u = blockIdx.x + i G);
 //   * the next pair's inputs are copied into a second shared-memory buffer while
-//     the current pair is computed (double buffering, 81 KB per buffer): one
-//     thread issues 1-D bulk copies of the FP64 state tile and RK4 sum, the two
-//     16 KB slices of the combined Psi/Pi table Zt and the pair's Rt and Q rows
-//     (completion on an mbarrier per buffer); every thread copies one 16-byte
-//     chunk of each W tile with cp.async into a bank-swizzled layout;
+//     the current pair is computed (double buffering, 81 KB per buffer): lane 0
+//     of warps 0, 1 and 2 issue 1-D bulk copies of the FP64 state tile and RK4
+//     sum, the two 16 KB slices of the combined Psi/Pi table Zt and the pair's
+//     Rt and Q rows (completion on an mbarrier per buffer; one thread issuing
+//     all six took 0.37 us per pair, while the other warps waited for it);
+//     every thread copies one 16-byte chunk of each W tile with cp.async into a
+//     bank-swizzled layout;
 //   * G1 is staged once per CTA, not once per tile pair;
 //   * the table terms i g22 (Rtt[site mu2] - Rtt[site nu2]) + g22 (Qt[mu2] -
 //     Qt[nu2]) of the per-pair kernel are read as g22 (Zt[mu2] - Zt[nu2]), two
@@ -71,21 +73,31 @@ struct EpiPUnit {
     int Rb, Cb, t, u;
 };
 
-// one thread: bulk copies of a tile pair's state tiles, table slices and rows, completing on bar
+// bulk copies of a tile pair's state tiles, table slices and rows, completing on
+// bar, issued by lane 0 of warps 0, 1 and 2 in parallel (each bulk copy takes
+// about 0.06 us to issue).  Warp 0's single arrival carries the whole byte
+// count, so the phase completes only when it has happened and every copy has
+// landed, in whatever order the warps run (the transaction count may go
+// below zero meanwhile).
 __device__ __forceinline__ void epip_issue_bulk(const SymDev &s, int k, const EpiPUnit &un, EpiPBuf &b, uint64_t *bar)
 {
     constexpr int n = 32, n2 = n * n, n3 = n2 * n;
     const bool diag = un.Rb == un.Cb;
     const uint32_t tile = kTB * kTB * sizeof(double2);
-    mbar_expect_tx(bar, tile * (1 + (k > 0) + 2 * !diag) + s.d.Ns * sizeof(double2) + n * sizeof(double2));
-    bulk_load(b.Yc, s.Yc + (long long)un.u * (kTB * kTB), tile, bar);
-    if (k > 0) bulk_load(b.Ac, s.Ac + (long long)un.u * (kTB * kTB), tile, bar);
-    if (!diag) {
-        bulk_load(b.Zm, s.d.Zt + un.t * n3 + un.Rb * n2, tile, bar);
-        bulk_load(b.Zn, s.d.Zt + un.t * n3 + un.Cb * n2, tile, bar);
+    const int w = threadIdx.x >> 5;
+    if (w == 0) {
+        mbar_expect_tx(bar, tile * (1 + (k > 0) + 2 * !diag) + s.d.Ns * sizeof(double2) + n * sizeof(double2));
+        bulk_load(b.Yc, s.Yc + (long long)un.u * (kTB * kTB), tile, bar);
+        if (k > 0) bulk_load(b.Ac, s.Ac + (long long)un.u * (kTB * kTB), tile, bar);
+    } else if (w == 1) {
+        if (!diag) {
+            bulk_load(b.Zm, s.d.Zt + un.t * n3 + un.Rb * n2, tile, bar);
+            bulk_load(b.Zn, s.d.Zt + un.t * n3 + un.Cb * n2, tile, bar);
+        }
+    } else {
+        bulk_load(b.Rt, s.d.Rt + (un.Rb * n + un.Cb) * s.d.Ns, s.d.Ns * sizeof(double2), bar);
+        bulk_load(b.Qr, s.d.Q + un.t * n3 + (un.Cb * n + un.Rb) * n, n * sizeof(double2), bar);
     }
-    bulk_load(b.Rt, s.d.Rt + (un.Rb * n + un.Cb) * s.d.Ns, s.d.Ns * sizeof(double2), bar);
-    bulk_load(b.Qr, s.d.Q + un.t * n3 + (un.Cb * n + un.Rb) * n, n * sizeof(double2), bar);
 }
 
 // every thread: its 16-byte chunk (source offset src, swizzled destination dst)
@@ -184,7 +196,7 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     grid_dep_wait();
     {
         const EpiPUnit un = units[0];
-        if (tid == 0) epip_issue_bulk(s, k, un, buf[0], &bar[0]);
+        if ((tid & 31) == 0 && tid < 96) epip_issue_bulk(s, k, un, buf[0], &bar[0]);
         epip_issue_w(un.t ? Wt1 : Wt0, un, buf[0], wdst, wsrc);
         cp_async_commit();
     }
@@ -193,7 +205,7 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
             // buffer (i + 1) & 1 was last read by pair i - 1, before the barrier after its K pass
             const EpiPUnit un1 = units[i + 1];
             EpiPBuf &b1 = buf[(i + 1) & 1];
-            if (tid == 0) epip_issue_bulk(s, k, un1, b1, &bar[(i + 1) & 1]);
+            if ((tid & 31) == 0 && tid < 96) epip_issue_bulk(s, k, un1, b1, &bar[(i + 1) & 1]);
             epip_issue_w(un1.t ? Wt1 : Wt0, un1, b1, wdst, wsrc);
             cp_async_commit();
             cp_async_wait<1>();
