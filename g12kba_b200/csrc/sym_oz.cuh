@@ -502,17 +502,25 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                 mbar_arrive(&acc_empty[b]);
                 named_sync(1, Sh::EPI);
                 float *Wg = s.W + t * 2 * s.n4;
+                // four consecutive entries of a W row per thread (one 16-byte store)
+                constexpr int QR = NN * NN / 4;           // 16-byte chunks per W row
+                constexpr int RPP = Sh::EPI / QR;         // W rows per pass
+                static_assert(Sh::EPI % QR == 0 && (Sh::CPT * 2) % RPP == 0, "W row passes");
+                const int q = et % QR, rsel = et / QR;
+                const int r0 = 4 * q, mu2 = r0 / NN, mu1 = r0 % NN;
 #pragma unroll 2
-                for (int sp = 0; sp < Sh::CPT * 2; ++sp) {
-                    const int slot = sp >> 1, part = sp & 1;
+                for (int sp0 = 0; sp0 < Sh::CPT * 2; sp0 += RPP) {
+                    const int sp = sp0 + rsel, slot = sp >> 1, part = sp & 1;
                     const int ps = tile_p(i, g, slot);
                     float *Wrow = Wg + ((long long)tile_c(i, g, slot) * 2 + part) * n2;
-#pragma unroll
-                    for (int r = et; r < NN * NN; r += Sh::EPI) {
-                        const int mu1 = r % NN, mu2 = r / NN;
-                        Wrow[r] = S[(slot * NN + mu2) * Sh::S_LD + part * NN + mu1] +
-                                  S[(ps * NN + mu1) * Sh::S_LD + part * NN + mu2];
-                    }
+                    float4 v;
+                    const float *a = S + (slot * NN + mu2) * Sh::S_LD + part * NN + mu1;
+                    const float *b = S + (ps * NN + mu1) * Sh::S_LD + part * NN + mu2;
+                    v.x = a[0] + b[0];
+                    v.y = a[1] + b[Sh::S_LD];
+                    v.z = a[2] + b[2 * Sh::S_LD];
+                    v.w = a[3] + b[3 * Sh::S_LD];
+                    *reinterpret_cast<float4 *>(Wrow + r0) = v;
                 }
                 named_sync(1, Sh::EPI);
             }
