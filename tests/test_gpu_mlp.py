@@ -161,7 +161,14 @@ def test_gradient_block_and_split_step(torch, learned):
         ge = _relf(g_host, a.grads())
         assert ge <= GRAD_TOL, ge
         da, db = a.get_params() - p0, b.get_params() - p0
-        assert _relf(db, da) <= 1e-2, _relf(db, da)
+        # Adam's first step is lr g / (|g| + eps) per entry: where |g| is near zero
+        # its sign follows the summation order of the atomics, so the update of those
+        # entries may differ by 2 lr; compare the entries with a gradient that is not
+        # negligible (at least half of them)
+        gmag = np.abs(g_host)
+        keep = gmag > 1e-3 * gmag.max()
+        assert keep.mean() > 0.5, keep.mean()
+        assert _relf(db[keep], da[keep]) <= 1e-2, _relf(db[keep], da[keep])
     off, parts = 0, []
     for l in range(4):
         for cnt in (dims[l] * dims[l + 1], dims[l + 1]):
