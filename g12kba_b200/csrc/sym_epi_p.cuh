@@ -53,13 +53,6 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait()
@@ -133,7 +126,7 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     __shared__ int site[n];
     __shared__ double wtab[n];  // pair weight by site distance m: U (m = 0), V_m (m <= nv), 0
     __shared__ EpiPUnit units[kEpiPMaxUnits];
-    __shared__ __align__(8) uint64_t bar[kEpiPEJ];
+    __shared__ __align__(8) uint64_t bar[2];  // one per input buffer
     const int tid = threadIdx.x;
     const int nu = (2 * s.npairs - int(blockIdx.x) + G - 1) / G;
     if (nu <= 0) return;

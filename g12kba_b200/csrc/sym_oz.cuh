@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
             mbar_init(&acc_full[q], 1);
             mbar_init(&acc_empty[q], Sh::EPI);
         }
-        mbar_init(b_ready, Sh::EPI);
+        mbar_init(b_ready, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // c values and partner slots of this CTA's first tiles (independent loads)
@@ -441,15 +441,16 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
             // the digits of h and their row scales, written by k_prep
             grid_dep_wait();
             const int et = tid - 320;  // 0 .. EPI-1
-            {
-                const uint4 *bsrc = reinterpret_cast<const uint4 *>(s.d.ozb);
-                for (int i = et; i < kOz2Digits * Sh::B_BYTES / 16; i += Sh::EPI)
-                    reinterpret_cast<uint4 *>(Bd)[i] = bsrc[i];
-                const float *sbsrc = reinterpret_cast<const float *>(s.d.ozb + kOz2Digits * Sh::B_BYTES);
-                for (int j = et; j < Sh::N; j += Sh::EPI) sB[j] = sbsrc[j];
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_arrive(b_ready);
+            if (et == 0) {
+                // one bulk copy of the digit tiles of h (cudaMalloc'd, so 16-byte
+                // aligned; B_BYTES and N * 4 are multiples of 16) and one of the row scales
+                mbar_expect_tx(b_ready, kOz2Digits * Sh::B_BYTES + Sh::N * 4);
+                bulk_load(Bd, s.d.ozb, kOz2Digits * Sh::B_BYTES, b_ready);
+                bulk_load(sB, s.d.ozb + kOz2Digits * Sh::B_BYTES, Sh::N * 4, b_ready);
             }
+            // the row scales sB are read below: wait for the copy once (bounded; a
+            // time-out makes every epilogue warp vote to leave at the first tile)
+            const bool b_ok = mbar_wait(b_ready, 0);
             // warp (quadrant q, column group cg) reads TMEM lanes 32q..32q+31,
             // columns cg*CW .. cg*CW+CW-1 of every level
             const int ew = warp - 10;
@@ -462,7 +463,7 @@ __global__ void __launch_bounds__(Oz2Shape<NN>::THREADS, 1) k_sym_gemm_oz2(SymDe
                 const int tile = blockIdx.x + i * gridDim.x;
                 const int t = tile / s.gemm_tiles, g = tile % s.gemm_tiles;
                 // the epilogue warps leave together (they share a named barrier)
-                const bool w = __all_sync(0xffffffffu, mbar_wait(&acc_full[b], (i >> 1) & 1));
+                const bool w = __all_sync(0xffffffffu, b_ok && mbar_wait(&acc_full[b], (i >> 1) & 1));
                 if (lane == 0) vote[ew] = w ? 1 : 0;
                 named_sync(1, Sh::EPI);
                 bool all = true;
