@@ -49,8 +49,8 @@ EVICT_BYTES = 160 << 20
 # DRAM bytes (read + write) per launch of the top kernels at n = 32, from one
 # `ncu --set full` capture each (the profiles/ summaries give the command).
 TOP_KERNEL_DRAM_BYTES = {
-    "k_sym_gemm_oz2": 16860928.0,
-    "k_sym_epi": 36916480.0,
+    "k_sym_gemm_oz2": 16856320.0,
+    "k_sym_epi": 37164288.0,
     "k_apply_tc<cols+epilogue>": 170896896.0,
 }
 
