@@ -105,6 +105,16 @@ __device__ __forceinline__ void step_begin_body(const Dev &d)
     __shared__ long long s_step;
     __shared__ int s_act, s_rec;
     const int tid = threadIdx.x;
+    const int n = d.n;
+    // this thread's first entries of G1, loaded while thread 0 reads the step
+    // counter and the schedule (they do not depend on them)
+    constexpr int kPre = 4;
+    double2 pre[kPre];
+#pragma unroll
+    for (int q = 0; q < kPre; ++q) {
+        const int x = tid + q * int(blockDim.x);
+        pre[q] = x < n * n ? d.Y1[x] : make_double2(0.0, 0.0);
+    }
     if (tid == 0) {
         const long long s = *d.counter;
         const int act = (*d.status == 0) && (s < *d.limit);
@@ -117,7 +127,6 @@ __device__ __forceinline__ void step_begin_body(const Dev &d)
         if (tid == 0) *d.active = 0;
         return;
     }
-    const int n = d.n;
     const long long s = s_step;
     {
         // this step's scalars, one word per thread
@@ -126,8 +135,16 @@ __device__ __forceinline__ void step_begin_body(const Dev &d)
         for (int w = tid; w < int(sizeof(StepP) / 4); w += blockDim.x) dst[w] = src[w];
     }
     double2 *tr = d.traj + (s % d.traj_cap) * d.n2;
+#pragma unroll
+    for (int q = 0; q < kPre; ++q) {
+        const int x = tid + q * int(blockDim.x);
+        if (x < n * n) {
+            d.G1t0[x] = pre[q];
+            if (s_rec) tr[x] = pre[q];
+        }
+    }
 #pragma unroll 4
-    for (int x = tid; x < n * n; x += blockDim.x) {
+    for (int x = tid + kPre * int(blockDim.x); x < n * n; x += blockDim.x) {
         const double2 v = d.Y1[x];
         d.G1t0[x] = v;
         if (s_rec) tr[x] = v;

@@ -184,12 +184,16 @@ __global__ void __launch_bounds__(kEpiPThreads, 1) k_sym_epi_p(SymDev s, int k)
     int sk[kEpiPEJ];
 #pragma unroll
     for (int j = 0; j < kEpiPEJ; ++j) sk[j] = site[w + kEpiPWarps * j];
-    // W comes from the GEMM launched just before this kernel, the tables from
-    // k_prep before it (G1 was complete before k_prep started)
+    // W comes from the GEMM launched just before this kernel: wait for it.  The
+    // first pair's state tiles (the previous stage's epilogue) and tables
+    // (k_prep) are fetched before that: both kernels have completed by the time
+    // any CTA of this one runs, which is on an SM that a finished GEMM CTA left
+    // (one 200 KB GEMM CTA per SM; each waited for k_prep before it finished).
+    // G1 was complete before k_prep started.
+    if ((tid & 31) == 0 && tid < 96) epip_issue_bulk(s, k, units[0], buf[0], &bar[0]);
     grid_dep_wait();
     {
         const EpiPUnit un = units[0];
-        if ((tid & 31) == 0 && tid < 96) epip_issue_bulk(s, k, un, buf[0], &bar[0]);
         epip_issue_w(un.t ? Wt1 : Wt0, un, buf[0], wdst, wsrc);
         cp_async_commit();
     }
