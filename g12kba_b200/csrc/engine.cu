@@ -31,6 +31,8 @@ struct LaunchCfg {
     size_t ab_smem, cd_smem, prep_smem, g1_smem;
     dim3 apply_grid;
     int prep_blocks, g1_blocks;
+    int prep_wide_blocks;    // k_prep_wide (mixed engine, n = 32)
+    size_t prep_wide_smem;
     int steps_per_graph;
 };
 
@@ -230,15 +232,28 @@ void enqueue_apply(const LaunchCfg &lc, const Dev &d, int k, cudaStream_t s, int
     }
 }
 
+// The stage tables.  On the mixed engine at n = 32 in 16-warp blocks: 66 blocks
+// instead of 264 leave SMs free, so that the digit GEMM (launched
+// programmatically after it) starts its first CTAs, those with a fourth tile,
+// while k_prep runs (a GEMM CTA does not fit beside a k_prep block).
+inline void enqueue_prep(const LaunchCfg &lc, const Dev &d, int k, cudaStream_t s, bool mixed_path)
+{
+    if (mixed_path && d.n == 32)
+        k_prep_wide<<<lc.prep_wide_blocks, kPrepWarpsWide * 32, lc.prep_wide_smem, s>>>(d, k);
+    else
+        k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, s>>>(d, k);
+}
+
 // One RK4 step.  k_g1 of stage k only feeds k_prep of stage k+1, so it runs
 // on a side branch (s2) concurrently with the two-body kernels of stage k.
 void enqueue_step(g12_ctx *ctx, const Dev &d, cudaStream_t s)
 {
     const LaunchCfg &lc = ctx->lc;
     k_step_begin<<<1, 256, 0, s>>>(d);
+    const bool mixed_path = ctx->prec != G12_PREC_FP64 && d.gate && mixed_fuses_g1(ctx->mixed);
     for (int k = 0; k < 4; ++k) {
-        k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, s>>>(d, k);
-        if (ctx->prec != G12_PREC_FP64 && d.gate && mixed_fuses_g1(ctx->mixed)) {
+        enqueue_prep(lc, d, k, s, mixed_path);
+        if (mixed_path) {
             // digit GEMM, then the epilogue with the G1 side as extra blocks of
             // its launch (two launches per stage after k_prep).  (Running
             // k_prep's table blocks on a side stream beside the GEMM was
@@ -561,6 +576,8 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     lc.apply_grid = dim3(unsigned((n2 + lc.ab.NB - 1) / lc.ab.NB), 2, 1);
     lc.prep_blocks = prep_blocks(n2);
     lc.prep_smem = prep_smem();
+    lc.prep_wide_blocks = prep_blocks<kPrepWarpsWide>(n2);
+    lc.prep_wide_smem = prep_smem<kPrepWarpsWide>();
     lc.g1_blocks = g1_blocks(n2);
     lc.g1_smem = g1_smem(n2);
     lc.steps_per_graph = n <= 8 ? 8 : (n <= 32 ? 4 : 1);
@@ -575,6 +592,8 @@ extern "C" int g12_create(const g12_params *p, int32_t precision, int32_t device
     if (!ck(ctx, cudaFuncSetAttribute(k_apply<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.ab_smem)), "attr") ||
         !ck(ctx, cudaFuncSetAttribute(k_apply<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.cd_smem)), "attr") ||
         !ck(ctx, cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.prep_smem)), "attr") ||
+        !ck(ctx, cudaFuncSetAttribute(k_prep_wide, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.prep_wide_smem)),
+            "attr") ||
         !ck(ctx, cudaFuncSetAttribute(k_g1, cudaFuncAttributeMaxDynamicSharedMemorySize, int(lc.g1_smem)), "attr"))
         return fail(G12_ERR_CUDA);
     if (precision != G12_PREC_FP64) {
@@ -901,9 +920,9 @@ extern "C" int32_t g12_kernel_times(g12_ctx *ctx, int32_t nsteps, double *avg_ms
     for (int s = 0; s < nsteps; ++s) {
         timed(0, [&] { k_step_begin<<<1, 256, 0, ctx->s>>>(d); });
         for (int k = 0; k < 4; ++k) {
-            timed(1, [&] { k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, ctx->s>>>(d, k); });
             // the digit-GEMM path runs the G1 side inside its epilogue launch
             const bool fused = ctx->prec != G12_PREC_FP64 && d.gate && mixed_fuses_g1(ctx->mixed);
+            timed(1, [&] { enqueue_prep(lc, d, k, ctx->s, fused); });
             if (!fused) timed(2, [&] { k_g1<<<lc.g1_blocks, kG1Threads, lc.g1_smem, ctx->s>>>(d, k); });
             if (!d.gate) continue;
             if (ctx->prec == G12_PREC_FP64) {

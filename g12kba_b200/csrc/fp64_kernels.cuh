@@ -223,10 +223,25 @@ __device__ __forceinline__ double2 h_entry(const Dev &d, const double2 *G, const
 // with d.Zt set, their combination Zt[t][r][b][a] = i Rt[a][b][r % Ns] + Q[t][a][b][r]
 // (the Psi and Pi factors that the epilogue multiplies by the same G1 entry).
 constexpr int kPrepWarps = 4;
+// k_prep_wide (the mixed engine at n = 32): the same work in 16-warp blocks,
+// 66 of them, which leave 82 SMs free for the digit GEMM's first CTAs
+constexpr int kPrepWarpsWide = 16;
 
-__host__ __device__ inline int prep_pair_blocks(long long n2) { return int((n2 + kPrepWarps - 1) / kPrepWarps); }
-inline int prep_blocks(long long n2) { return prep_pair_blocks(n2) + int((n2 + kPrepWarps * 32 - 1) / (kPrepWarps * 32)); }
-inline size_t prep_smem() { return size_t(kPrepWarps) * 4 * kMaxN * sizeof(double2); }
+template <int W = kPrepWarps>
+__host__ __device__ inline int prep_pair_blocks(long long n2)
+{
+    return int((n2 + W - 1) / W);
+}
+template <int W = kPrepWarps>
+inline int prep_blocks(long long n2)
+{
+    return prep_pair_blocks<W>(n2) + int((n2 + W * 32 - 1) / (W * 32));
+}
+template <int W = kPrepWarps>
+inline size_t prep_smem()
+{
+    return size_t(W) * 4 * kMaxN * sizeof(double2);
+}
 
 // Exact bf16 digits of the real form of h^T for the tcgen05 digit GEMM of the
 // symmetric engine (sym_oz.cuh, k_sym_gemm_oz2), written once per stage by the
@@ -287,19 +302,22 @@ __device__ __forceinline__ void prep_h_part(const Dev &d, int k, int hb)
         hv = h_entry(d, G, sm_h, int(x / n), int(x % n), st);
         d.h[x] = hv;
     }
-    if (d.ozb) h_digits(d, hv, int(x));
+    if (d.ozb && x < n2) h_digits(d, hv, int(x));  // whole warps (n2 is a multiple of 32 with digits)
 }
 
+template <int W>
 __device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx);
 
+template <int W = kPrepWarps>
 __device__ __forceinline__ void prep_body(const Dev &d, int k, int bx)
 {
-    const int pair_blocks = prep_pair_blocks(d.n2);
+    const int pair_blocks = prep_pair_blocks<W>(d.n2);
     if (bx >= pair_blocks) prep_h_part(d, k, bx - pair_blocks);
-    else prep_pair_part(d, k, bx);
+    else prep_pair_part<W>(d, k, bx);
 }
 
-// the Psi, Pi and collision tables: one (alpha, beta) pair per warp
+// the Psi, Pi and collision tables: one (alpha, beta) pair per warp, W warps per block
+template <int W>
 __device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx)
 {
     if (!*d.active) return;
@@ -313,7 +331,7 @@ __device__ __forceinline__ void prep_pair_part(const Dev &d, int k, int bx)
     double2 *wDx = wE + kMaxN;               // n
     double2 *wDy = wDx + kMaxN;              // n
     double2 *wS = wDy + kMaxN;               // R / S, Ns entries
-    const long long pair = (long long)bx * kPrepWarps + warp;
+    const long long pair = (long long)bx * W + warp;
     if (pair >= n2) return;
     const int alpha = int(pair / n), beta = int(pair % n);
     const double U = st.U;
@@ -442,6 +460,12 @@ static __global__ void __launch_bounds__(kPrepWarps * 32) k_prep(Dev d, int k)
 {
     grid_dep_launch();  // the symmetric engine's GEMM may start its prologue
     prep_body(d, k, blockIdx.x);
+}
+
+static __global__ void __launch_bounds__(kPrepWarpsWide * 32) k_prep_wide(Dev d, int k)
+{
+    grid_dep_launch();
+    prep_body<kPrepWarpsWide>(d, k, blockIdx.x);
 }
 
 // G1 side of a stage (commutators.h:28-51, G1_G2_t_step.h:24-47) and the
