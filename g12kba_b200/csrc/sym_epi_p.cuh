@@ -11,7 +11,8 @@
 //     all six took 0.37 us per pair, while the other warps waited for it);
 //     every thread copies one 16-byte chunk of each W tile with cp.async into a
 //     bank-swizzled layout;
-//   * G1 is staged once per CTA, not once per tile pair;
+//   * G1 is staged once per CTA, not once per tile pair, and the first pair's
+//     bulk copies are issued before the wait for the GEMM (only W comes from it);
 //   * the table terms i g22 (Rtt[site mu2] - Rtt[site nu2]) + g22 (Qt[mu2] -
 //     Qt[nu2]) of the per-pair kernel are read as g22 (Zt[mu2] - Zt[nu2]), two
 //     shared-memory reads instead of four L2 reads per element;

@@ -174,7 +174,7 @@ __device__ __forceinline__ void named_sync(int id, int nthreads)
 //               staging -> W = T1 + e(T1)
 // so the loads of tile i+2, the digits and products of tile i+1 and the
 // epilogue of tile i overlap.  The digits of h come from k_prep
-// (h_digits).  Every wait is bounded.
+// (h_digits), fetched by one bulk copy.  Every wait is bounded.
 constexpr int kOz2Digits = 4;     // digits per operand = accumulation levels
 constexpr int kOz2ListTiles = 8;  // tiles per CTA whose c / partner lists are staged in shared memory
 
