@@ -236,9 +236,11 @@ void enqueue_apply(const LaunchCfg &lc, const Dev &d, int k, cudaStream_t s, int
 // instead of 264 leave SMs free, so that the digit GEMM (launched
 // programmatically after it) starts its first CTAs, those with a fourth tile,
 // while k_prep runs (a GEMM CTA does not fit beside a k_prep block).
+inline bool prep_is_wide(bool mixed_path, const Dev &d) { return mixed_path && d.n == 32; }
+
 inline void enqueue_prep(const LaunchCfg &lc, const Dev &d, int k, cudaStream_t s, bool mixed_path)
 {
-    if (mixed_path && d.n == 32)
+    if (prep_is_wide(mixed_path, d))
         k_prep_wide<<<lc.prep_wide_blocks, kPrepWarpsWide * 32, lc.prep_wide_smem, s>>>(d, k);
     else
         k_prep<<<lc.prep_blocks, kPrepWarps * 32, lc.prep_smem, s>>>(d, k);
@@ -881,6 +883,9 @@ extern "C" const char *g12_kernel_name(const g12_ctx *ctx, int32_t kind)
     if (!ctx) return "";
     if (ctx->prec != G12_PREC_FP64 && kind >= 3) return mixed_kernel_name(ctx->mixed, kind - 3);
     if (kind < 0 || kind >= 5) return "";
+    if (kind == 1 &&
+        prep_is_wide(ctx->prec != G12_PREC_FP64 && ctx->d.gate && mixed_fuses_g1(ctx->mixed), ctx->d))
+        return "k_prep_wide";
     return ctx->lc.tc ? kFp64TcNames[kind] : kFp64Names[kind];
 }
 
