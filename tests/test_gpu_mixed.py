@@ -201,6 +201,30 @@ def test_bf16oz_config2_full_length(g12, gate):
     assert np.max(np.abs(pg - pr)) <= FULL_TOL * max(np.max(np.abs(pr)), np.max(np.abs(ref)))
 
 
+def test_bf16oz_config3_full_length(g12):
+    """The headline workload: Ns=16, Nb=2 (n=32), t2=0.3, U=1.5, EHM U/(1+r),
+    full quench 1.5 on Nq=4, dt=0.01, 10,000 steps from the plain FP64 engine's
+    switched state (the digit GEMM, k_prep_wide and the persistent epilogue
+    against plain FP64; on this model the plain engine stays on the physical
+    states).  G1 and dipole within the metric's 1e-6 over the whole run."""
+    p = g12.make_params(Ns=16, Nb=2, Nq=4, time_steps=10000, U=1.5, t1=1.0, t2=0.3, dt=0.01, EHM=True,
+                        v_law="inv", q_type="full", quench_strength=1.5)
+    T = g12.rk_iterations(p)
+    assert T == 10000
+    with g12.Context(p, "fp64") as ctx:
+        ctx.set_state(g12.make_G0(p))
+        ctx.adiabatic_switch()
+        S = ctx.get_state()
+        ref, rc0 = ctx.propagate(T)
+    with g12.Context(p, "bf16oz") as ctx:
+        ctx.set_state(*S)
+        got, rc1 = ctx.propagate(T)
+    assert rc0 == 0 and rc1 == 0
+    assert rel_err(got, ref) <= FULL_TOL, rel_err(got, ref)
+    pr, pg = g12.dipole(ref), g12.dipole(got)
+    assert np.max(np.abs(pg - pr)) <= FULL_TOL * max(np.max(np.abs(pr)), np.max(np.abs(ref)))
+
+
 @pytest.mark.parametrize("prec", ["fp64", "fp64sym"])
 def test_config2_unphysical_part_grows(g12, prec):
     """The observation behind the previous test: the exchange-antisymmetric
