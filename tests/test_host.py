@@ -172,6 +172,38 @@ def test_writers_match_reference_text(g12):
             assert open(os.path.join(d, name)).read() == open(os.path.join(mine, name)).read(), name
 
 
+def test_writers_g_format_wide_range(g12, tmp_path):
+    """The text writers format every value as the reference's streams do
+    (default precision 6, i.e. printf %g): values over the whole exponent range,
+    ties at the sixth significant digit, signed zeros, subnormals and integers;
+    and a 2-D file with more rows than one pass of the multithreaded writer (16
+    threads x 64-row blocks) and a ragged last pass, rows in order."""
+    rng = np.random.default_rng(11)
+    vals = np.concatenate([
+        rng.standard_normal(4000) * 10.0 ** rng.integers(-300, 300, 4000),
+        np.array([0.0, -0.0, 1.0, -1.0, 123456.5, 1234565.0, 0.1234565, 1e-5, 9.999995e-5, 1e16, 5e-324,
+                  1.7976931348623157e308]),
+        np.round(rng.standard_normal(500) * 1e6),
+    ])
+    rfile = tmp_path / "dipole.txt"
+    assert g12.lib().g12_write_rfile(str(rfile).encode(), vals.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                     vals.size) == 0
+    assert rfile.read_text() == "".join("%g\n" % v for v in vals)
+    T, n2 = 7, 2 * 16 * 64 + 5
+    z = (rng.standard_normal((T, n2)) + 1j * rng.standard_normal((T, n2))) * 10.0 ** rng.integers(-8, 8, (T, n2))
+    z = np.ascontiguousarray(z)
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        rc = g12.lib().g12_write_cfile2D(b"G1.txt", z.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), T, n2)
+    finally:
+        os.chdir(cwd)
+    assert rc == 0
+    for part, name in ((z.real, "real_G1.txt"), (z.imag, "imag_G1.txt")):
+        want = "".join("".join("%g " % part[i, j] for i in range(T)) + "\n" for j in range(n2))
+        assert (tmp_path / name).read_text() == want, name
+
+
 def test_ensemble_generator_is_seeded(g12):
     a = g12.ensemble_params(16)
     b = g12.ensemble_params(16)
